@@ -1,0 +1,368 @@
+"""Benchmark: forward + backward point*texel throughput of the visibility-masked env-map shader.
+
+Workload (per rank): 70,000 points x 16x32 env map with 512 packed visibility bits per point
+(Bernoulli(0.7)), specular on, one forward (bruteforce_specularvisibility_shader_forward2) and
+one backward (..._backward2) per step.  Metric = points * texels / (t_fwd + t_bwd).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+
+Timing: W untimed warm-up steps; then K steps, each bracketed by CUDA events on the launching
+stream; a 256 MiB buffer larger than the 126 MB L2 is rewritten between timed steps (outside the
+events).  Multi-GPU (torchrun): every rank shades its own 70k points (weak scaling) and the
+env-map gradients are summed over ranks with one NCCL all-reduce (the path's only exchange);
+the reported time is the max over ranks.
+
+``--impl reference`` times the CPU restatement of the reference's sum (the reference has no
+CPU path of its own) on the host cores, on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd point*texel/s (70k pts, 16x32 env, 512-bit visibility)"
+UNIT = "point*texel/s"
+CONFIG_NAME = "vis-70k"
+
+# Algorithmic FP32-pipe instructions per (point, texel) pair (FMA = 1), see DESIGN.md.
+INSTR_FWD_VIS = 57
+INSTR_BWD_VIS = 148
+FP32_LANES_PER_SM = 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if not self.rows:
+            return None
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def committed_traffic():
+    """DRAM bytes per launch of the adjoint kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "bwd_kernel_vis70k_ncu.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU leg (oracle port): reference arm and cpu_baseline
+# ------------------------------------------------------------------------------------------------
+
+def cpu_port_throughput(inp, target_s=8.0, max_points=None):
+    """FP32 oracle (C++ transcription of the reference sum) fwd+bwd on all host threads over a
+    bounded sample of the workload's points; returns (point*texel/s, sample description, threads)."""
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    flags = orc.flags_for("specularvisibility2")
+    HW = inp.HW
+    gs = inp.grad_shading.numpy()
+    gw = inp.grad_diffuse_shading.numpy()
+    n = 512
+    total_pairs, total_t, npts = 0, 0.0, 0
+    while True:
+        pts = np.arange(n) % inp.P
+        t0 = time.perf_counter()
+        orc.forward(inp, flags, dtype=np.float32, nthreads=threads, points=pts)
+        orc.backward(inp, flags, gs, gw, dtype=np.float32, nthreads=threads, points=pts)
+        dt = time.perf_counter() - t0
+        total_pairs += n * HW
+        total_t += dt
+        npts += n
+        if total_t >= target_s or (max_points and npts >= max_points):
+            break
+        n = int(min(max(n * 2, 512), inp.P))
+    desc = (f"{npts} points x {HW} texels fwd+bwd (FP32 oracle, visibility), {threads} threads, "
+            f"{total_t:.1f} s")
+    return total_pairs / total_t, desc, threads
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from diff_envshade_b200 import workloads as wl
+    inp = wl.make_config(CONFIG_NAME)
+    per_step_s = max(2.0, 60.0 / max(args.steps + args.warmup, 1))
+    vals = []
+    desc = threads = None
+    for i in range(args.warmup + args.steps):
+        v, desc, threads = cpu_port_throughput(inp, target_s=per_step_s)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    pairs = inp.P * inp.HW
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": pairs / value * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"{CONFIG_NAME}: 70000 points x 16x32 env, 512-bit visibility, specular on",
+                   "note": "reference has no CPU path: C++ FP32 restatement of its sum (oracle port)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    import diff_envshade_b200 as des
+    from diff_envshade_b200 import workloads as wl
+
+    c = wl.CONFIGS[CONFIG_NAME]
+    inp_host = wl.make_inputs(c["P"], c["H"], c["W"], c["seed"] + 1000 * rank, sigma=c["sigma"], rough=c["rough"],
+                              vis_p=c["vis_p"])
+    d = inp_host.to(dev)
+    P, HW = d.P, d.HW
+    vis = (d.face_vertex_list, d.nearest_triangle_id, d.barycentric_coord, d.visibility)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        sh, wh = des.bruteforce_specularvisibility_shader_forward2(
+            d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness, d.envmap, d.light2obj_rotmat, *vis, True)
+        g = des.bruteforce_specularvisibility_shader_backward2(
+            d.grad_shading, d.grad_diffuse_shading, d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness,
+            d.envmap, d.light2obj_rotmat, *vis, True)
+        if pg is not None:
+            pg.all_reduce(g[5])
+        return sh, wh, g
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    kf = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    kb = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    for i in range(K):
+        flush.fill_(float(i))
+        ev[i][0].record()
+        des.set_timing_events(kf[i][0].cuda_event, kf[i][1].cuda_event)
+        sh, wh = des.bruteforce_specularvisibility_shader_forward2(
+            d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness, d.envmap, d.light2obj_rotmat, *vis, True)
+        des.set_timing_events(kb[i][0].cuda_event, kb[i][1].cuda_event)
+        g = des.bruteforce_specularvisibility_shader_backward2(
+            d.grad_shading, d.grad_diffuse_shading, d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness,
+            d.envmap, d.light2obj_rotmat, *vis, True)
+        des.set_timing_events(0, 0)
+        if pg is not None:
+            pg.all_reduce(g[5])
+        ev[i][1].record()
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    fwd_ms = [a.elapsed_time(b) for a, b in kf]
+    bwd_ms = [a.elapsed_time(b) for a, b in kb]
+    total_ms = float(np.sum(step_ms))
+    if pg is not None:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / K
+    value = world * P * HW / (ms_per_step * 1e-3)
+
+    # ---- end-to-end through the public autograd API, host buffers, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        hp = inp_host.pin()
+        names = ["normal", "view_dir", "albedo", "specular_albedo", "roughness", "envmap", "light2obj_rotmat",
+                 "face_vertex_list", "nearest_triangle_id", "barycentric_coord", "visibility", "grad_shading",
+                 "grad_diffuse_shading"]
+        h2d = sum(getattr(hp, k).numel() * getattr(hp, k).element_size() for k in names)
+        out_host = None
+
+        def e2e_step():
+            nonlocal out_host
+            t = {k: getattr(hp, k).to(dev, non_blocking=True) for k in names}
+            for k in ("normal", "view_dir", "albedo", "specular_albedo", "roughness", "envmap"):
+                t[k].requires_grad_(True)
+            sh, wh = des.shade(t["normal"], t["view_dir"], t["albedo"], t["specular_albedo"], t["roughness"],
+                               t["envmap"], t["light2obj_rotmat"],
+                               visibility=(t["face_vertex_list"], t["nearest_triangle_id"], t["barycentric_coord"],
+                                           t["visibility"]))
+            torch.autograd.backward([sh, wh], [t["grad_shading"], t["grad_diffuse_shading"]])
+            if pg is not None:
+                pg.all_reduce(t["envmap"].grad)
+            outs = [sh.detach(), wh.detach()] + [t[k].grad for k in ("normal", "view_dir", "albedo",
+                                                                     "specular_albedo", "roughness", "envmap")]
+            if out_host is None:
+                out_host = [torch.empty(o.shape, dtype=o.dtype, pin_memory=True) for o in outs]
+            for o, h in zip(outs, out_host):
+                h.copy_(o, non_blocking=True)
+            return sum(o.numel() * o.element_size() for o in outs)
+
+        for _ in range(args.warmup):
+            d2h = e2e_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(K):
+            d2h = e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        if pg is not None:
+            t = torch.tensor([e2e_ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * P * HW / (e2e_ms / K * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / K, "api": "diff_envshade_b200.shade + "
+               "torch.autograd.backward (pinned host inputs, H2D + fwd + bwd + D2H of every output)"}
+
+    # ---- roofline of the dominant kernel (fused adjoint) and of the forward kernel
+    peaks = measured_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_tinst = sms * FP32_LANES_PER_SM * sm_max * 1e6 / 1e12
+    bwd_avg = float(np.mean(bwd_ms)) * 1e-3
+    fwd_avg = float(np.mean(fwd_ms)) * 1e-3
+    ach_bwd = P * HW * INSTR_BWD_VIS / bwd_avg / 1e12
+    ach_fwd = P * HW * INSTR_FWD_VIS / fwd_avg / 1e12
+    roofline = {
+        "bound": "fp32", "kernel": "des_bwd_kernel<diffuse,specular,visibility> (fused adjoint)",
+        "achieved": ach_bwd, "peak": peak_tinst, "unit": "T FP32-pipe instr/s", "frac": ach_bwd / peak_tinst,
+        "traffic": committed_traffic(),
+        "peak_source": f"derived: {sms} SMs x {FP32_LANES_PER_SM} FP32 lanes x {sm_max:.0f} MHz "
+                       "(sm_max_mhz of MEASURED_PEAKS.json; no measured FP32 peak exists)",
+        "work": f"{INSTR_BWD_VIS} FP32-pipe instr per point*texel pair x {P}x{HW} pairs per launch",
+        "kernel_ms": bwd_avg * 1e3,
+        "forward": {"kernel_ms": fwd_avg * 1e3, "achieved": ach_fwd, "frac": ach_fwd / peak_tinst,
+                    "work": f"{INSTR_FWD_VIS} instr/pair"},
+    }
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, desc, threads = cpu_port_throughput(inp_host, target_s=10.0)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded normals/views/materials, lognormal env, Bernoulli(0.7) bits)",
+            "config": {"workload": f"{CONFIG_NAME}: {P} points x {d.envmap.shape[1]}x{d.envmap.shape[2]} env, "
+                                   f"{d.visibility.shape[0] * 32}-bit visibility, specular on, fwd+bwd",
+                       "points_per_rank": P, "texels": HW, "parallelism": f"dp{world}" if world > 1 else "single",
+                       "l2": "256 MiB buffer rewritten between timed steps (outside the timed events)"},
+            "gpu_launches": 5 * K,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+            "fwd_ms": float(np.mean(fwd_ms)), "bwd_ms": float(np.mean(bwd_ms)),
+        }
+        print(json.dumps(line))
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

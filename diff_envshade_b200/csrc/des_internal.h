@@ -1,0 +1,82 @@
+// Internal declarations shared by the kernel translation units and the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "diff_envshade_b200.h"
+
+namespace des {
+
+constexpr int kMaxThreads = 512;  // largest CTA of the shading kernels (16 warps)
+constexpr int kChunk = 2048;      // texels of the table staged in shared memory at once
+constexpr size_t kCtrlBytes = 256;
+
+// control words at the start of every workspace
+enum : int { kCtrlTileCounter = 0, kCtrlError = 1 };
+
+// Kernel parameters (passed by value in the launch).
+struct ShadeParams {
+  int64_t P;
+  int HWpad, chunk, ntiles;
+  int N_face, N_vertex;
+  const float* normal;
+  const float* view;
+  const float* albedo;
+  const float* spec;
+  const float* rough;
+  const int32_t* faces;
+  const int64_t* tri;
+  const float* bary;
+  const uint32_t* vis;
+  const float4* table;  // [HWpad][2] texel records
+  bool clamp;
+  bool env_in_smem;
+  unsigned* ctrl;
+  // forward outputs
+  float* shading;
+  float* white;
+  // backward inputs / outputs
+  const float* g_shading;
+  const float* g_white;
+  float* g_normal;
+  float* g_view;
+  float* g_albedo;
+  float* g_spec;
+  float* g_rough;
+  double* env_partial;  // [grid][3][HWpad]
+};
+
+struct LaunchPlan {
+  int HWpad, chunk, ntiles, nw;
+  bool env_in_smem;
+  size_t smem;
+  int sms, max_smem;
+};
+
+struct ShadeCall {
+  const des_shade_args* args;
+  unsigned flags;
+  bool backward;
+  float* shading;
+  float* white;
+  const float* g_shading;
+  const float* g_white;
+  float* g_normal;
+  float* g_view;
+  float* g_albedo;
+  float* g_spec;
+  float* g_rough;
+  float* g_envmap;
+  void* workspace;
+  size_t workspace_bytes;
+};
+
+LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev);
+size_t workspace_bytes(const LaunchPlan& lp, bool backward, int grid);
+int shade_grid(const LaunchPlan& lp, unsigned flags, bool backward, bool vis);
+int launch_shade(const ShadeCall& call, des_stream_t stream);
+int launch_texel_table(int H, int W, const float* R, float* out, des_stream_t stream);
+void set_timing_events(cudaEvent_t start, cudaEvent_t stop);
+
+}  // namespace des

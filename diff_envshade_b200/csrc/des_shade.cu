@@ -1,0 +1,834 @@
+// Brute-force environment-map shading on B200 (sm_100a): forward sum and fused adjoint.
+//
+// Work decomposition (all shading kernels):
+//  * a tile is 32 consecutive points, one point per lane of a warp;
+//  * a CTA of NW warps processes one tile at a time, warp w integrating the tile over its own
+//    contiguous run of 32-texel visibility slots, so the NW warps split the texel axis;
+//  * CTAs are persistent: the grid is sized to the resident capacity of the device, and CTAs
+//    pull tiles from a device counter (the next tile index is fetched one tile ahead);
+//  * the texel table {rotated direction, d_omega, radiance, d_omega/pi} of the whole env map is
+//    staged once per CTA in shared memory (in chunks of kChunk texels for very large maps).
+// Per-point partial sums of the NW warps are combined through shared memory at the end of a
+// tile in a fixed order, so every per-point output is deterministic.
+//
+// Env-map gradient: per 8-texel group the 32 lanes' contributions are summed by a transposing
+// butterfly of warp shuffles (each of 8 lanes ends up holding one texel), added into a per-CTA
+// FP64 accumulator in shared memory, written once per CTA, and summed over CTAs in FP64 by
+// des_env_reduce_kernel.
+//
+// Reference correspondence (zjumsj/diff_envshade, bruteforce_shader.cu):
+//   forward     = BruteForce{Diffuse,Specular,SpecularClamp}ShaderKernel_Forward (231, 532, 1040),
+//                 BruteForceSpecular{,Visibility}ShaderKernel_Forward2 (1554, 2068)
+//   backward    = the matching *_Backward / *_Backward2 point-gradient kernels (318, 689, 1197,
+//                 1701, 2248) fused with the *_BackwardEnvmap* env-gradient kernels (435, 888,
+//                 1396, 1928, 2508) into one pass.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+
+#include "des_math.cuh"
+#include "des_internal.h"
+#include "diff_envshade_b200.h"
+
+namespace des {
+
+// ------------------------------------------------------------------------------------------
+// Texel table
+// ------------------------------------------------------------------------------------------
+
+// One launch per call: rec[2t] = (l'x, l'y, l'z, d_omega), rec[2t+1] = (L0, L1, L2, d_omega/pi)
+// for t < H*W, zeros for the padding up to a multiple of 32.  Also resets the control words of
+// the workspace (tile counter, error word) for the kernel that follows on the same stream.
+// `export4` (optional) receives (x, y, z, d_omega) per texel for des_texel_table.
+__global__ void des_table_kernel(int H, int W, int HWpad, const float* __restrict__ R,
+                                 const float* __restrict__ env, float4* __restrict__ rec,
+                                 float* __restrict__ export4, unsigned* __restrict__ ctrl) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0 && ctrl != nullptr) {
+    ctrl[kCtrlTileCounter] = 0u;
+    ctrl[kCtrlError] = 0u;
+  }
+  if (t >= HWpad) return;
+  const int HW = H * W;
+  if (t < HW) {
+    int ix = t % W;
+    int iy = t / W;
+    iy = H - 1 - iy;  // LEFT_TOP_AS_ORIGIN (reference config.h:11): memory row 0 is the top row
+    float m[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) m[i] = R[i];
+    const float3 l = rotate3(m, texel_direction(iy, ix, W, H));
+    const float dw = texel_delta_omega(iy, W, H);
+    if (rec != nullptr) {
+      rec[2 * t] = make_float4(l.x, l.y, l.z, dw);
+      rec[2 * t + 1] = make_float4(env[t], env[HW + t], env[2 * HW + t], dw * kInvPiF);
+    }
+    if (export4 != nullptr) {
+      export4[4 * t + 0] = l.x;
+      export4[4 * t + 1] = l.y;
+      export4[4 * t + 2] = l.z;
+      export4[4 * t + 3] = dw;
+    }
+  } else if (rec != nullptr) {
+    rec[2 * t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    rec[2 * t + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Shared pieces of the shading kernels
+// ------------------------------------------------------------------------------------------
+
+// Copies texels [base, base + len) of the table into shared memory (len a multiple of 32).
+__device__ __forceinline__ void stage_table(float4* __restrict__ s_tab, const float4* __restrict__ g_tab,
+                                            int base, int len) {
+  for (int i = threadIdx.x; i < 2 * len; i += blockDim.x) s_tab[i] = g_tab[2 * base + i];
+}
+
+struct PointGeom {
+  float nx, ny, nz;  // normal (zeroed for inactive lanes: then no texel passes n.l > 0)
+  float vx, vy, vz;  // view direction
+  int v0, v1, v2;    // visibility vertices
+  float c0, c1, c2;  // barycentric weights
+};
+
+// Loads a lane's normal / view / visibility vertices.  Out-of-range triangle or vertex ids set
+// the workspace error bit and make the point inactive (it then shades to zero).
+template <bool VIS>
+__device__ __forceinline__ PointGeom load_geom(const ShadeParams& p, int64_t pid, bool valid, bool need_view) {
+  PointGeom g;
+  g.nx = g.ny = g.nz = 0.f;
+  g.vx = g.vy = g.vz = 0.f;
+  g.v0 = g.v1 = g.v2 = 0;
+  g.c0 = g.c1 = g.c2 = 0.f;
+  if (!valid) return g;
+  g.nx = p.normal[3 * pid];
+  g.ny = p.normal[3 * pid + 1];
+  g.nz = p.normal[3 * pid + 2];
+  if (need_view) {
+    g.vx = p.view[3 * pid];
+    g.vy = p.view[3 * pid + 1];
+    g.vz = p.view[3 * pid + 2];
+  }
+  if (VIS) {
+    const int64_t f = p.tri[pid];
+    bool ok = (f >= 0) && (f < p.N_face);
+    if (ok) {
+      g.v0 = p.faces[f];
+      g.v1 = p.faces[f + p.N_face];
+      g.v2 = p.faces[f + 2 * (int64_t)p.N_face];
+      ok = (g.v0 >= 0) && (g.v0 < p.N_vertex) && (g.v1 >= 0) && (g.v1 < p.N_vertex) && (g.v2 >= 0) &&
+           (g.v2 < p.N_vertex);
+    }
+    if (!ok) {
+      atomicOr(&p.ctrl[kCtrlError], 1u);
+      g.v0 = g.v1 = g.v2 = 0;
+      g.nx = g.ny = g.nz = 0.f;
+    }
+    g.c0 = p.bary[pid];
+    g.c1 = p.bary[pid + p.P];
+    g.c2 = p.bary[pid + 2 * p.P];
+  }
+  // backface clamp (bruteforce_shader.cu:1111): the whole texel loop is skipped when n.v <= 0
+  if (p.clamp && !(dot3(g.nx, g.ny, g.nz, g.vx, g.vy, g.vz) > 0.f)) g.nx = g.ny = g.nz = 0.f;
+  return g;
+}
+
+__device__ __forceinline__ void load_vis_words(const ShadeParams& p, const PointGeom& g, bool valid, int slot,
+                                               uint32_t& w0, uint32_t& w1, uint32_t& w2) {
+  if (valid) {
+    const uint32_t* row = p.vis + (int64_t)slot * p.N_vertex;
+    w0 = __ldg(row + g.v0);
+    w1 = __ldg(row + g.v1);
+    w2 = __ldg(row + g.v2);
+  } else {
+    w0 = w1 = w2 = 0u;
+  }
+}
+
+// Per-point GGX constants (bruteforce_shader.cu:1601-1604 and G1_robust's view factor).
+struct SpecConst {
+  float alpha2, am1;  // alpha^2 = r^4 and alpha^2 - 1
+  float k, omk;       // k = (r+1)^2/8 and 1 - k
+  float invB;         // 1 / (max(n.v,0) (1-k) + k)
+  float nvp;          // max(n.v, 0)
+};
+
+__device__ __forceinline__ SpecConst spec_const(float r, const PointGeom& g) {
+  SpecConst s;
+  float a0 = r * r;
+  s.alpha2 = a0 * a0;
+  s.am1 = s.alpha2 - 1.f;
+  float a1 = r + 1.f;
+  s.k = (a1 * a1) / 8.f;
+  s.omk = 1.f - s.k;
+  s.nvp = fmaxf(dot3(g.vx, g.vy, g.vz, g.nx, g.ny, g.nz), 0.f);
+  s.invB = 1.f / fmaf(s.nvp, s.omk, s.k);
+  return s;
+}
+
+// ------------------------------------------------------------------------------------------
+// Forward
+// ------------------------------------------------------------------------------------------
+
+template <bool DIFF, bool SPEC, bool VIS>
+__global__ void __launch_bounds__(kMaxThreads, 1) des_fwd_kernel(const ShadeParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* s_tab = reinterpret_cast<float4*>(smem_raw);
+  float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)p.chunk * 32);
+  __shared__ int s_next[2];
+
+  const int NW = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nchunks = (p.HWpad + p.chunk - 1) / p.chunk;
+  const bool need_view = SPEC || p.clamp;
+
+  if (nchunks == 1) {
+    stage_table(s_tab, p.table, 0, p.HWpad);
+    __syncthreads();
+  }
+
+  int tile = blockIdx.x;
+  int it = 0;
+  while (tile < p.ntiles) {
+    if (threadIdx.x == 0) s_next[it & 1] = (int)gridDim.x + (int)atomicAdd(&p.ctrl[kCtrlTileCounter], 1u);
+
+    const int64_t pid = (int64_t)tile * 32 + lane;
+    const bool valid = pid < p.P;
+    const PointGeom g = load_geom<VIS>(p, pid, valid, need_view);
+    SpecConst sc;
+    if (SPEC) sc = spec_const(valid ? p.rough[pid] : 0.f, g);
+
+    float D0 = 0.f, D1 = 0.f, D2 = 0.f;  // sum L * diffuse weight  (white diffuse shading)
+    float S0 = 0.f, S1 = 0.f, S2 = 0.f;  // sum L * specular weight
+
+    for (int c = 0; c < nchunks; ++c) {
+      const int cbase = c * p.chunk;
+      const int clen = min(p.chunk, p.HWpad - cbase);
+      if (nchunks > 1) {
+        __syncthreads();
+        stage_table(s_tab, p.table, cbase, clen);
+        __syncthreads();
+      }
+      const int nsl = clen >> 5;
+      const int sl0 = (warp * nsl) / NW, sl1 = ((warp + 1) * nsl) / NW;
+      const int gslot0 = cbase >> 5;
+      uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
+      if (VIS && sl0 < sl1) load_vis_words(p, g, valid, gslot0 + sl0, n0, n1, n2);
+      for (int sl = sl0; sl < sl1; ++sl) {
+        uint32_t w0 = n0, w1 = n1, w2 = n2;
+        if (VIS) {
+          if (sl + 1 < sl1) load_vis_words(p, g, valid, gslot0 + sl + 1, n0, n1, n2);
+          // skip a 32-point x 32-texel tile that is fully occluded for every lane
+          if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
+        }
+        const float4* rec = s_tab + 2 * (sl << 5);
+#pragma unroll 1
+        for (int gq = 0; gq < 4; ++gq) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float4 A = rec[2 * (gq * 8 + j)];
+            const float4 B = rec[2 * (gq * 8 + j) + 1];
+            const float nl = dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z);
+            const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
+            const bool act = nl > 0.f;
+            if (DIFF) {
+              const float wd = act ? nl * B.w * vis : 0.f;
+              D0 = fmaf(B.x, wd, D0);
+              D1 = fmaf(B.y, wd, D1);
+              D2 = fmaf(B.z, wd, D2);
+            }
+            if (SPEC) {
+              const float hx = A.x + g.vx, hy = A.y + g.vy, hz = A.z + g.vz;
+              const float hh = fmaxf(dot3(hx, hy, hz, hx, hy, hz), kHalfVecFloor);
+              const float ri = rsqrt_approx(hh);
+              const float nh = dot3(g.nx, g.ny, g.nz, hx, hy, hz) * ri;
+              const float lh = dot3(A.x, A.y, A.z, hx, hy, hz) * ri;
+              const float a = 1.f - __saturatef(lh);
+              const float a2 = a * a;
+              const float F = fmaf(a2 * a2 * a, 1.f - kR0, kR0);
+              const float G = nl * rcp_approx(fmaf(nl, sc.omk, sc.k)) * sc.invB;
+              const float tt = fmaf(nh * nh, sc.am1, 1.f);
+              const float D = sc.alpha2 * rcp_approx(fmaxf(kPiF * tt * tt, kThres));
+              const float tmp = F * G * D * 0.25f;
+              const float ws = (act && tmp > 0.f) ? tmp * A.w * vis : 0.f;
+              S0 = fmaf(B.x, ws, S0);
+              S1 = fmaf(B.y, ws, S1);
+              S2 = fmaf(B.z, ws, S2);
+            }
+          }
+          if (VIS) {
+            w0 >>= 8;
+            w1 >>= 8;
+            w2 >>= 8;
+          }
+        }
+      }
+    }
+
+    // combine the NW texel ranges in warp order
+    float* red = s_red + warp * 6 * 32 + lane;
+    red[0] = D0; red[32] = D1; red[64] = D2;
+    red[96] = S0; red[128] = S1; red[160] = S2;
+    __syncthreads();
+    if (warp == 0 && valid) {
+      float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      for (int w = 0; w < NW; ++w) {
+        const float* r = s_red + w * 6 * 32 + lane;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) acc[q] += r[q * 32];
+      }
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {
+        float out = 0.f;
+        if (DIFF) out = p.albedo[3 * pid + ch] * acc[ch];
+        if (SPEC) out = fmaf(p.spec[3 * pid + ch], acc[3 + ch], out);
+        p.shading[3 * pid + ch] = out;
+        if (p.white != nullptr) p.white[3 * pid + ch] = acc[ch];
+      }
+    }
+    __syncthreads();
+    tile = s_next[it & 1];
+    ++it;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Backward (point gradients + env-map gradient in one pass)
+// ------------------------------------------------------------------------------------------
+
+// Transposing butterfly: e[j] (j = 0..7) per lane -> every lane holds the 32-lane sum of texel
+// 4*b4 + 2*b3 + b2 of its lane id (b4 = bit 4, ...), identical in lanes that differ in bits 0-1.
+__device__ __forceinline__ float butterfly8(const float (&e)[8], int lane) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  float x[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float keep = b4 ? e[i + 4] : e[i];
+    const float send = b4 ? e[i] : e[i + 4];
+    x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  float y[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const float keep = b3 ? x[i + 2] : x[i];
+    const float send = b3 ? x[i] : x[i + 2];
+    y[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  float z;
+  {
+    const float keep = b2 ? y[1] : y[0];
+    const float send = b2 ? y[0] : y[1];
+    z = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  return z;
+}
+
+template <bool DIFF, bool SPEC, bool VIS>
+__global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadeParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* s_tab = reinterpret_cast<float4*>(smem_raw);
+  double* s_env = reinterpret_cast<double*>(smem_raw + (size_t)p.chunk * 32);  // [3][chunk], single chunk
+  float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)p.chunk * 32 + (p.env_in_smem ? (size_t)p.chunk * 24 : 0));
+  __shared__ int s_next[2];
+
+  constexpr int NACC = 15;
+  const int NW = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nchunks = (p.HWpad + p.chunk - 1) / p.chunk;
+  const bool need_view = SPEC || p.clamp;
+  // env-gradient accumulator of this CTA: [3][HWpad] doubles (shared memory if it fits)
+  double* env_acc = p.env_in_smem ? s_env : p.env_partial + (size_t)blockIdx.x * 3 * p.HWpad;
+  const int env_ld = p.env_in_smem ? p.chunk : p.HWpad;
+  {
+    const int n = 3 * env_ld;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) env_acc[i] = 0.0;
+  }
+  if (nchunks == 1) stage_table(s_tab, p.table, 0, p.HWpad);
+  __syncthreads();
+
+  int tile = blockIdx.x;
+  int it = 0;
+  while (tile < p.ntiles) {
+    if (threadIdx.x == 0) s_next[it & 1] = (int)gridDim.x + (int)atomicAdd(&p.ctrl[kCtrlTileCounter], 1u);
+
+    const int64_t pid = (int64_t)tile * 32 + lane;
+    const bool valid = pid < p.P;
+    const PointGeom g = load_geom<VIS>(p, pid, valid, need_view);
+    // incoming gradients folded with the albedos (bruteforce_shader.cu:2585-2588)
+    float gd0 = 0.f, gd1 = 0.f, gd2 = 0.f, gs0 = 0.f, gs1 = 0.f, gs2 = 0.f;
+    SpecConst sc;
+    if (valid) {
+      const float g0 = p.g_shading[3 * pid], g1 = p.g_shading[3 * pid + 1], g2 = p.g_shading[3 * pid + 2];
+      if (DIFF) {
+        gd0 = g0 * p.albedo[3 * pid];
+        gd1 = g1 * p.albedo[3 * pid + 1];
+        gd2 = g2 * p.albedo[3 * pid + 2];
+        if (p.g_white != nullptr) {
+          gd0 += p.g_white[3 * pid];
+          gd1 += p.g_white[3 * pid + 1];
+          gd2 += p.g_white[3 * pid + 2];
+        }
+      }
+      if (SPEC) {
+        gs0 = g0 * p.spec[3 * pid];
+        gs1 = g1 * p.spec[3 * pid + 1];
+        gs2 = g2 * p.spec[3 * pid + 2];
+      }
+    }
+    if (SPEC) sc = spec_const(valid ? p.rough[pid] : 0.f, g);
+
+    float Da0 = 0.f, Da1 = 0.f, Da2 = 0.f;  // sum L * diffuse weight  -> g_albedo
+    float Sa0 = 0.f, Sa1 = 0.f, Sa2 = 0.f;  // sum L * specular weight -> g_specular_albedo
+    float gnx = 0.f, gny = 0.f, gnz = 0.f;
+    float gvx = 0.f, gvy = 0.f, gvz = 0.f;
+    float ga1 = 0.f, ga2 = 0.f, gbs = 0.f;  // d/d k, d/d alpha^2, sum of d/d b (G1 view factor)
+
+    for (int c = 0; c < nchunks; ++c) {
+      const int cbase = c * p.chunk;
+      const int clen = min(p.chunk, p.HWpad - cbase);
+      if (nchunks > 1) {
+        __syncthreads();
+        stage_table(s_tab, p.table, cbase, clen);
+        __syncthreads();
+      }
+      const int nsl = clen >> 5;
+      const int sl0 = (warp * nsl) / NW, sl1 = ((warp + 1) * nsl) / NW;
+      const int gslot0 = cbase >> 5;
+      const int ebase = p.env_in_smem ? 0 : cbase;
+      uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
+      if (VIS && sl0 < sl1) load_vis_words(p, g, valid, gslot0 + sl0, n0, n1, n2);
+      for (int sl = sl0; sl < sl1; ++sl) {
+        uint32_t w0 = n0, w1 = n1, w2 = n2;
+        if (VIS) {
+          if (sl + 1 < sl1) load_vis_words(p, g, valid, gslot0 + sl + 1, n0, n1, n2);
+          if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
+        }
+        const float4* rec = s_tab + 2 * (sl << 5);
+#pragma unroll 1
+        for (int gq = 0; gq < 4; ++gq) {
+          float wdj[8], wsj[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float4 A = rec[2 * (gq * 8 + j)];
+            const float4 B = rec[2 * (gq * 8 + j) + 1];
+            const float nl = dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z);
+            const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
+            const bool act = nl > 0.f;
+            wdj[j] = 0.f;
+            wsj[j] = 0.f;
+            if (DIFF) {
+              // Lambert adjoint (bruteforce_shader.cu:2413-2426)
+              const float wdv = act ? B.w * vis : 0.f;  // d_omega/pi * vis
+              const float wd = nl * wdv;
+              Da0 = fmaf(B.x, wd, Da0);
+              Da1 = fmaf(B.y, wd, Da1);
+              Da2 = fmaf(B.z, wd, Da2);
+              const float gdot = dot3(gd0, gd1, gd2, B.x, B.y, B.z) * wdv;
+              gnx = fmaf(gdot, A.x, gnx);
+              gny = fmaf(gdot, A.y, gny);
+              gnz = fmaf(gdot, A.z, gnz);
+              wdj[j] = wd;
+            }
+            if (SPEC) {
+              const float hx = A.x + g.vx, hy = A.y + g.vy, hz = A.z + g.vz;
+              const float hh = fmaxf(dot3(hx, hy, hz, hx, hy, hz), kHalfVecFloor);
+              const float ri = rsqrt_approx(hh);
+              const float nh = dot3(g.nx, g.ny, g.nz, hx, hy, hz) * ri;
+              const float lh = dot3(A.x, A.y, A.z, hx, hy, hz) * ri;
+              const float a = 1.f - __saturatef(lh);
+              const float a2 = a * a;
+              const float a4 = a2 * a2;
+              const float F = fmaf(a4 * a, 1.f - kR0, kR0);
+              const float ia = rcp_approx(fmaf(nl, sc.omk, sc.k));
+              const float Ga = nl * ia;
+              const float G = Ga * sc.invB;
+              const float nh2 = nh * nh;
+              const float tt = fmaf(nh2, sc.am1, 1.f);
+              const float t2 = kPiF * tt * tt;
+              const float itm = rcp_approx(fmaxf(t2, kThres));
+              const float D = sc.alpha2 * itm;
+              const float tmp = F * G * D * 0.25f;
+              const float wsv = (act && tmp > 0.f) ? A.w * vis : 0.f;  // d_omega * vis
+              const float ws = tmp * wsv;
+              Sa0 = fmaf(B.x, ws, Sa0);
+              Sa1 = fmaf(B.y, ws, Sa1);
+              Sa2 = fmaf(B.z, ws, Sa2);
+              wsj[j] = ws;
+              // d shading / d tmp, then split into F, G, D (bruteforce_shader.cu:2436-2445)
+              const float q = dot3(gs0, gs1, gs2, B.x, B.y, B.z) * wsv * 0.25f;
+              const float gF = q * (G * D);
+              const float gG = q * (F * D);
+              const float gD = q * (F * G);
+              // Fresnel adjoint (bruteforce_shader.cu:155-159)
+              const float gch = (lh >= 0.f && lh <= 1.f) ? (5.f * (kR0 - 1.f)) * gF * a4 : 0.f;
+              float ghx = gch * A.x, ghy = gch * A.y, ghz = gch * A.z;
+              // Schlick-Smith adjoint, light side (bruteforce_shader.cu:173-201); the view side is
+              // linear in a per-point factor and is applied once per point after the loop
+              const float gA = gG * sc.invB;
+              const float ia2 = ia * ia;
+              const float gdln = gA * sc.k * ia2;
+              gnx = fmaf(gdln, A.x, gnx);
+              gny = fmaf(gdln, A.y, gny);
+              gnz = fmaf(gdln, A.z, gnz);
+              ga1 = fmaf(gA * ia2, fmaf(nl, nl, -nl), ga1);
+              gbs = fmaf(-gA * Ga, sc.invB, gbs);
+              // GGX NDF adjoint (bruteforce_shader.cu:212-227); 1/t = pi t / (pi t^2)
+              ga2 = fmaf(gD, itm, ga2);
+              const float gt = (t2 > kThres) ? (-2.f * kPiF) * sc.alpha2 * gD * tt * itm * itm : 0.f;
+              ga2 = fmaf(nh2, gt, ga2);
+              const float gdnh = 2.f * gt * sc.am1 * nh;
+              const float hnx = hx * ri, hny = hy * ri, hnz = hz * ri;
+              gnx = fmaf(gdnh, hnx, gnx);
+              gny = fmaf(gdnh, hny, gny);
+              gnz = fmaf(gdnh, hnz, gnz);
+              ghx = fmaf(gdnh, g.nx, ghx);
+              ghy = fmaf(gdnh, g.ny, ghy);
+              ghz = fmaf(gdnh, g.nz, ghz);
+              // normalize adjoint (bruteforce_shader.cu:63-71) and h = l + v -> v
+              const float hg = dot3(hnx, hny, hnz, ghx, ghy, ghz);
+              gvx = fmaf(fmaf(-hnx, hg, ghx), ri, gvx);
+              gvy = fmaf(fmaf(-hny, hg, ghy), ri, gvy);
+              gvz = fmaf(fmaf(-hnz, hg, ghz), ri, gvz);
+            }
+          }
+          if (VIS) {
+            w0 >>= 8;
+            w1 >>= 8;
+            w2 >>= 8;
+          }
+          // env-map gradient of these 8 texels: per lane e = gd * wd + gs * ws, summed over lanes
+          const int t0 = ebase + (sl << 5) + gq * 8;
+          const int jsel = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+          float e[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) e[j] = fmaf(gs0, wsj[j], gd0 * wdj[j]);
+          const float y0 = butterfly8(e, lane);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) e[j] = fmaf(gs1, wsj[j], gd1 * wdj[j]);
+          const float y1 = butterfly8(e, lane);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) e[j] = fmaf(gs2, wsj[j], gd2 * wdj[j]);
+          const float y2 = butterfly8(e, lane);
+          if ((lane & 3) == 0) {
+            double* acc = env_acc + t0 + jsel;
+            acc[0] += (double)y0;
+            acc[env_ld] += (double)y1;
+            acc[2 * env_ld] += (double)y2;
+          }
+        }
+      }
+    }
+
+    // combine the NW texel ranges in warp order, then finish the per-point chain rule
+    float* red = s_red + warp * NACC * 32 + lane;
+    red[0 * 32] = Da0; red[1 * 32] = Da1; red[2 * 32] = Da2;
+    red[3 * 32] = Sa0; red[4 * 32] = Sa1; red[5 * 32] = Sa2;
+    red[6 * 32] = gnx; red[7 * 32] = gny; red[8 * 32] = gnz;
+    red[9 * 32] = gvx; red[10 * 32] = gvy; red[11 * 32] = gvz;
+    red[12 * 32] = ga1; red[13 * 32] = ga2; red[14 * 32] = gbs;
+    __syncthreads();
+    if (warp == 0 && valid) {
+      float acc[NACC];
+#pragma unroll
+      for (int q = 0; q < NACC; ++q) acc[q] = 0.f;
+      for (int w = 0; w < NW; ++w) {
+        const float* r = s_red + w * NACC * 32 + lane;
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) acc[q] += r[q * 32];
+      }
+      float n_x = acc[6], n_y = acc[7], n_z = acc[8];
+      float v_x = acc[9], v_y = acc[10], v_z = acc[11];
+      float g_rough = 0.f;
+      if (SPEC) {
+        // view side of the Schlick-Smith adjoint (bruteforce_shader.cu:194-200)
+        const float gdvn = acc[14] * sc.omk;
+        if (sc.nvp > 0.f) {
+          v_x = fmaf(gdvn, g.nx, v_x);
+          v_y = fmaf(gdvn, g.ny, v_y);
+          v_z = fmaf(gdvn, g.nz, v_z);
+          n_x = fmaf(gdvn, g.vx, n_x);
+          n_y = fmaf(gdvn, g.vy, n_y);
+          n_z = fmaf(gdvn, g.vz, n_z);
+        }
+        const float gk = fmaf(acc[14], 1.f - sc.nvp, acc[12]);
+        // roughness chain rule (bruteforce_shader.cu:2501-2502)
+        const float r = p.rough[pid];
+        g_rough = acc[13] * 4.f * r * r * r;
+        g_rough += gk * (1.f + r) / 4.f;
+      }
+      p.g_normal[3 * pid] = n_x;
+      p.g_normal[3 * pid + 1] = n_y;
+      p.g_normal[3 * pid + 2] = n_z;
+      const float g0 = p.g_shading[3 * pid], g1 = p.g_shading[3 * pid + 1], g2 = p.g_shading[3 * pid + 2];
+      if (p.g_albedo != nullptr) {
+        p.g_albedo[3 * pid] = DIFF ? g0 * acc[0] : 0.f;
+        p.g_albedo[3 * pid + 1] = DIFF ? g1 * acc[1] : 0.f;
+        p.g_albedo[3 * pid + 2] = DIFF ? g2 * acc[2] : 0.f;
+      }
+      if (p.g_spec != nullptr) {
+        p.g_spec[3 * pid] = SPEC ? g0 * acc[3] : 0.f;
+        p.g_spec[3 * pid + 1] = SPEC ? g1 * acc[4] : 0.f;
+        p.g_spec[3 * pid + 2] = SPEC ? g2 * acc[5] : 0.f;
+      }
+      if (p.g_view != nullptr) {
+        p.g_view[3 * pid] = SPEC ? v_x : 0.f;
+        p.g_view[3 * pid + 1] = SPEC ? v_y : 0.f;
+        p.g_view[3 * pid + 2] = SPEC ? v_z : 0.f;
+      }
+      if (p.g_rough != nullptr) p.g_rough[pid] = g_rough;
+    }
+    __syncthreads();
+    tile = s_next[it & 1];
+    ++it;
+  }
+
+  // publish this CTA's env-gradient partial (FP64)
+  if (p.env_in_smem) {
+    double* dst = p.env_partial + (size_t)blockIdx.x * 3 * p.HWpad;
+    for (int i = threadIdx.x; i < 3 * p.HWpad; i += blockDim.x) dst[i] = s_env[i];
+  }
+}
+
+// Deterministic FP64 sum of the per-CTA env-gradient partials: g_env[c][t] = sum_b partial[b][c][t].
+// Block = 32 columns x 32 rows; rows stride over the partials, then a fixed-order tree over rows.
+__global__ void __launch_bounds__(1024) des_env_reduce_kernel(const double* __restrict__ partial, int nparts,
+                                                              int HW, int HWpad, float* __restrict__ g_env) {
+  __shared__ double s[32][33];
+  const int x = threadIdx.x, y = threadIdx.y;
+  const int k = blockIdx.x * 32 + x;  // index into [3][HWpad]
+  const int n = 3 * HWpad;
+  double acc = 0.0;
+  if (k < n) {
+    for (int b = y; b < nparts; b += 32) acc += partial[(size_t)b * n + k];
+  }
+  s[y][x] = acc;
+  __syncthreads();
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    if (y < off) s[y][x] += s[y + off][x];
+    __syncthreads();
+  }
+  if (y == 0 && k < n) {
+    const int c = k / HWpad, t = k - c * HWpad;
+    if (t < HW) g_env[(size_t)c * HW + t] = (float)s[0][x];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Host-side launch logic
+// ------------------------------------------------------------------------------------------
+
+namespace {
+
+struct DeviceInfo {
+  int sms = 0;
+  int max_smem_optin = 0;
+};
+
+DeviceInfo device_info(int dev) {
+  static std::mutex mu;
+  static DeviceInfo cache[64];
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64) return DeviceInfo{};
+  if (cache[dev].sms == 0) {
+    cudaDeviceGetAttribute(&cache[dev].sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&cache[dev].max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  }
+  return cache[dev];
+}
+
+template <typename K>
+int occupancy(K kernel, int threads, size_t smem) {
+  // opt in to the dynamic shared memory this launch needs (idempotent)
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess) return 0;
+  return nb;
+}
+
+using KernelFn = void (*)(const ShadeParams);
+
+template <template <bool, bool, bool> class Sel>
+KernelFn pick(bool diff, bool spec, bool vis) {
+  if (diff) {
+    if (spec) return vis ? Sel<true, true, true>::fn() : Sel<true, true, false>::fn();
+    return vis ? Sel<true, false, true>::fn() : Sel<true, false, false>::fn();
+  }
+  return vis ? Sel<false, true, true>::fn() : Sel<false, true, false>::fn();
+}
+template <bool D, bool S, bool V>
+struct FwdSel {
+  static KernelFn fn() { return des_fwd_kernel<D, S, V>; }
+};
+template <bool D, bool S, bool V>
+struct BwdSel {
+  static KernelFn fn() { return des_bwd_kernel<D, S, V>; }
+};
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev) {
+  LaunchPlan lp{};
+  const DeviceInfo di = device_info(dev);
+  const int HW = H * W;
+  lp.HWpad = (HW + 31) / 32 * 32;
+  lp.chunk = std::min(lp.HWpad, kChunk);
+  lp.ntiles = (int)((P + 31) / 32);
+  lp.env_in_smem = backward && (lp.HWpad <= kChunk);
+  // texel-split width: more warps per tile when there are few tiles to spread over the SMs
+  const int nslots = lp.chunk / 32;
+  int nw = (lp.ntiles >= 2 * std::max(di.sms, 1)) ? 8 : 16;
+  while (nw > 1 && nw > nslots) nw >>= 1;
+  lp.nw = nw;
+  const int nacc = backward ? 15 : 6;
+  lp.smem = (size_t)lp.chunk * 32 + (lp.env_in_smem ? (size_t)lp.chunk * 24 : 0) + (size_t)nw * nacc * 32 * 4;
+  lp.sms = di.sms;
+  lp.max_smem = di.max_smem_optin;
+  return lp;
+}
+
+size_t workspace_bytes(const LaunchPlan& lp, bool backward, int grid) {
+  size_t off = kCtrlBytes;
+  off += align_up((size_t)lp.HWpad * 32, 256);  // texel table
+  if (backward) off += align_up((size_t)std::max(grid, 1) * 3 * lp.HWpad * sizeof(double), 256);
+  return off;
+}
+
+// Persistent grid: every CTA resident at once, never more CTAs than tiles.
+int shade_grid(const LaunchPlan& lp, unsigned flags, bool backward, bool vis) {
+  const bool diff = flags & DES_DIFFUSE, spec = flags & DES_SPECULAR;
+  if (!diff && !spec) return 1;
+  KernelFn k = backward ? pick<BwdSel>(diff, spec, vis) : pick<FwdSel>(diff, spec, vis);
+  const int occ = occupancy(k, lp.nw * 32, lp.smem);
+  if (occ <= 0) return 0;
+  return std::max(1, std::min(lp.ntiles, occ * lp.sms));
+}
+
+namespace {
+std::atomic<cudaEvent_t> g_timing_start{nullptr};
+std::atomic<cudaEvent_t> g_timing_stop{nullptr};
+}  // namespace
+
+void set_timing_events(cudaEvent_t start, cudaEvent_t stop) {
+  g_timing_start.store(start);
+  g_timing_stop.store(stop);
+}
+
+int launch_shade(const ShadeCall& call, des_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  const des_shade_args& a = *call.args;
+  const bool diff = call.flags & DES_DIFFUSE, spec = call.flags & DES_SPECULAR;
+  const bool vis = a.visibility != nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DES_ERR_CUDA;
+  LaunchPlan lp = plan_launch(a.P, a.H, a.W, call.backward, dev);
+  if (lp.smem > (size_t)lp.max_smem) return DES_ERR_UNSUPPORTED;
+  const int grid = shade_grid(lp, call.flags, call.backward, vis);
+  if (grid <= 0) return DES_ERR_CUDA;
+  const size_t need = workspace_bytes(lp, call.backward, grid);
+  if (call.workspace == nullptr || call.workspace_bytes < need ||
+      (reinterpret_cast<uintptr_t>(call.workspace) & 255u) != 0)
+    return DES_ERR_WORKSPACE;
+
+  unsigned char* ws = static_cast<unsigned char*>(call.workspace);
+  unsigned* ctrl = reinterpret_cast<unsigned*>(ws);
+  float4* table = reinterpret_cast<float4*>(ws + kCtrlBytes);
+  double* env_partial = reinterpret_cast<double*>(ws + kCtrlBytes + align_up((size_t)lp.HWpad * 32, 256));
+
+  // texel table + control-word reset
+  {
+    const int threads = 256;
+    const int blocks = (lp.HWpad + threads - 1) / threads;
+    des_table_kernel<<<blocks, threads, 0, stream>>>(a.H, a.W, lp.HWpad, a.light2obj_rotmat, a.envmap, table,
+                                                     nullptr, ctrl);
+    if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+  }
+  if (a.P == 0) {
+    if (call.backward && call.g_envmap != nullptr)
+      if (cudaMemsetAsync(call.g_envmap, 0, sizeof(float) * 3 * (size_t)a.H * a.W, stream) != cudaSuccess)
+        return DES_ERR_CUDA;
+    return DES_OK;
+  }
+  if (!diff && !spec) {
+    // nothing to integrate: every output is zero (reference allocates zeros for disabled terms)
+    const size_t pb = sizeof(float) * 3 * (size_t)a.P;
+    cudaError_t e = cudaSuccess;
+    if (!call.backward) {
+      e = cudaMemsetAsync(call.shading, 0, pb, stream);
+      if (e == cudaSuccess && call.white) e = cudaMemsetAsync(call.white, 0, pb, stream);
+    } else {
+      float* outs[4] = {call.g_normal, call.g_view, call.g_albedo, call.g_spec};
+      for (float* o : outs)
+        if (o && e == cudaSuccess) e = cudaMemsetAsync(o, 0, pb, stream);
+      if (call.g_rough && e == cudaSuccess) e = cudaMemsetAsync(call.g_rough, 0, pb / 3, stream);
+      if (call.g_envmap && e == cudaSuccess)
+        e = cudaMemsetAsync(call.g_envmap, 0, sizeof(float) * 3 * (size_t)a.H * a.W, stream);
+    }
+    return e == cudaSuccess ? DES_OK : DES_ERR_CUDA;
+  }
+
+  ShadeParams prm{};
+  prm.P = a.P;
+  prm.HWpad = lp.HWpad;
+  prm.chunk = lp.chunk;
+  prm.ntiles = lp.ntiles;
+  prm.N_face = a.N_face;
+  prm.N_vertex = a.N_vertex;
+  prm.normal = a.normal;
+  prm.view = a.view_dir;
+  prm.albedo = a.albedo;
+  prm.spec = a.specular_albedo;
+  prm.rough = a.roughness;
+  prm.faces = a.face_vertex_list;
+  prm.tri = a.nearest_triangle_id;
+  prm.bary = a.barycentric_coord;
+  prm.vis = a.visibility;
+  prm.table = table;
+  prm.clamp = (call.flags & DES_CLAMP) != 0;
+  prm.ctrl = ctrl;
+  prm.shading = call.shading;
+  prm.white = call.white;
+  prm.g_shading = call.g_shading;
+  prm.g_white = call.g_white;
+  prm.g_normal = call.g_normal;
+  prm.g_view = call.g_view;
+  prm.g_albedo = call.g_albedo;
+  prm.g_spec = call.g_spec;
+  prm.g_rough = call.g_rough;
+  prm.env_partial = env_partial;
+  prm.env_in_smem = lp.env_in_smem;
+
+  KernelFn k = call.backward ? pick<BwdSel>(diff, spec, vis) : pick<FwdSel>(diff, spec, vis);
+  cudaEvent_t ev0 = g_timing_start.load(), ev1 = g_timing_stop.load();
+  if (ev0 != nullptr && ev1 != nullptr) cudaEventRecord(ev0, stream);
+  k<<<grid, lp.nw * 32, lp.smem, stream>>>(prm);
+  if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+  if (ev0 != nullptr && ev1 != nullptr) cudaEventRecord(ev1, stream);
+
+  if (call.backward && call.g_envmap != nullptr) {
+    const dim3 rb(32, 32);
+    const int rg = (3 * lp.HWpad + 31) / 32;
+    des_env_reduce_kernel<<<rg, rb, 0, stream>>>(env_partial, grid, a.H * a.W, lp.HWpad, call.g_envmap);
+    if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+  }
+  return DES_OK;
+}
+
+int launch_texel_table(int H, int W, const float* R, float* out, des_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  const int HWpad = (H * W + 31) / 32 * 32;
+  const int threads = 256;
+  des_table_kernel<<<(HWpad + threads - 1) / threads, threads, 0, stream>>>(H, W, HWpad, R, nullptr, nullptr, out,
+                                                                            nullptr);
+  return cudaGetLastError() == cudaSuccess ? DES_OK : DES_ERR_CUDA;
+}
+
+}  // namespace des

@@ -1,0 +1,408 @@
+// Torch extension: the reference's pybind operator surface (zjumsj/diff_envshade bindings.cpp:6-19,
+// gsface_shader.h:1-118) over the C ABI of libdes_b200.
+//
+// Each function keeps the reference's name, argument order, tensor layouts and return order.
+// Differences, all deliberate:
+//  * shapes are checked (the reference has "TODO: shape check", bruteforce_shader.cu:3289);
+//  * float inputs must be float32 (the reference admits half/double in CHECK_IS_FLOATING and then
+//    fails inside data_ptr<float>(), so the accepted set is the same);
+//  * kernels run on the current PyTorch stream, not the legacy default stream;
+//  * with DES_CHECK_INDICES=1 in the environment, out-of-range triangle/vertex ids raise after
+//    the call (this synchronises the stream); by default such points shade to zero.
+#include <ATen/cuda/CUDAContext.h>
+#include <c10/cuda/CUDAGuard.h>
+#include <torch/extension.h>
+
+#include <cstdlib>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "diff_envshade_b200.h"
+
+namespace {
+
+using torch::Tensor;
+
+void check_f32(const Tensor& x, const char* name) {
+  TORCH_CHECK(x.device().is_cuda(), name, " must be a CUDA tensor");
+  TORCH_CHECK(x.is_contiguous(), name, " must be a contiguous tensor");
+  TORCH_CHECK(x.scalar_type() == at::ScalarType::Float, name, " must be a float32 tensor");
+}
+void check_i32(const Tensor& x, const char* name) {
+  TORCH_CHECK(x.device().is_cuda(), name, " must be a CUDA tensor");
+  TORCH_CHECK(x.is_contiguous(), name, " must be a contiguous tensor");
+  TORCH_CHECK(x.scalar_type() == at::ScalarType::Int, name, " must be an int tensor");
+}
+void check_i64(const Tensor& x, const char* name) {
+  TORCH_CHECK(x.device().is_cuda(), name, " must be a CUDA tensor");
+  TORCH_CHECK(x.is_contiguous(), name, " must be a contiguous tensor");
+  TORCH_CHECK(x.scalar_type() == at::ScalarType::Long, name, "must be an long tensor");
+}
+void check_rows(const Tensor& x, int64_t rows, int64_t cols, const char* name) {
+  TORCH_CHECK(x.dim() == 2 && x.size(0) == rows && x.size(1) == cols, name, " must have shape [", rows, ", ", cols,
+              "], got ", x.sizes());
+}
+
+bool check_indices_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("DES_CHECK_INDICES");
+    return e != nullptr && std::string(e) == "1";
+  }();
+  return on;
+}
+
+void raise_status(int st) {
+  if (st == DES_OK) return;
+  if (st == DES_ERR_UNSUPPORTED) throw std::runtime_error("Channel number not supported!");
+  TORCH_CHECK(false, "diff_envshade_b200: ", des_status_string(st));
+}
+
+struct Common {
+  int64_t P, C;
+  int H, W;
+};
+
+// Shapes shared by every shading op.  Returns sizes in the reference's convention
+// (P = normal.size(0), C = albedo.size(1), H, W = envmap.size(1, 2)).
+Common common_checks(const Tensor& normal, const Tensor& albedo, const Tensor& envmap, const Tensor& R) {
+  check_f32(normal, "normal");
+  check_f32(albedo, "albedo");
+  check_f32(envmap, "envmap");
+  check_f32(R, "light2obj_rotmat");
+  TORCH_CHECK(normal.dim() == 2 && normal.size(1) == 3, "normal must have shape [P, 3], got ", normal.sizes());
+  TORCH_CHECK(albedo.dim() == 2, "albedo must have shape [P, C], got ", albedo.sizes());
+  TORCH_CHECK(envmap.dim() == 3, "envmap must have shape [C, H, W], got ", envmap.sizes());
+  TORCH_CHECK(R.numel() == 9, "light2obj_rotmat must have 9 elements (3x3), got ", R.sizes());
+  Common c;
+  c.P = normal.size(0);
+  c.C = albedo.size(1);
+  c.H = (int)envmap.size(1);
+  c.W = (int)envmap.size(2);
+  if (c.C != 3) throw std::runtime_error("Channel number not supported!");
+  check_rows(albedo, c.P, c.C, "albedo");
+  TORCH_CHECK(envmap.size(0) == c.C, "envmap must have C = albedo.size(1) = ", c.C, " channels");
+  return c;
+}
+
+void spec_checks(const Common& c, const Tensor& view, const Tensor& spec, const Tensor& rough) {
+  check_f32(view, "view_dir");
+  check_f32(spec, "specular_albedo");
+  check_f32(rough, "roughness");
+  check_rows(view, c.P, 3, "view_dir");
+  check_rows(spec, c.P, c.C, "specular_albedo");
+  TORCH_CHECK(rough.numel() == c.P, "roughness must have P = ", c.P, " elements (P x 1), got ", rough.sizes());
+}
+
+struct VisArgs {
+  int N_face, N_vertex, N_slot;
+};
+VisArgs vis_checks(const Common& c, const Tensor& faces, const Tensor& tri, const Tensor& bary, const Tensor& vis) {
+  check_i32(faces, "face_vertex_list");
+  check_i64(tri, "nearest_triangle_id");
+  check_f32(bary, "barycentric_coord");
+  check_i32(vis, "visibility");
+  TORCH_CHECK(faces.dim() == 2 && faces.size(0) == 3, "face_vertex_list must have shape [3, N_face], got ",
+              faces.sizes());
+  TORCH_CHECK(tri.numel() == c.P, "nearest_triangle_id must have P = ", c.P, " elements");
+  check_rows(bary, 3, c.P, "barycentric_coord");
+  TORCH_CHECK(vis.dim() == 2, "visibility must have shape [N_slot, N_vertex], got ", vis.sizes());
+  VisArgs v;
+  v.N_face = (int)faces.size(1);
+  v.N_vertex = (int)vis.size(1);
+  v.N_slot = (int)vis.size(0);
+  const int64_t need = ((int64_t)c.H * c.W + 31) / 32;
+  TORCH_CHECK(v.N_slot >= need, "visibility needs at least ceil(H*W/32) = ", need, " slots (rows), got ", v.N_slot);
+  if (c.P > 0) {
+    TORCH_CHECK(v.N_face > 0, "face_vertex_list is empty");
+    TORCH_CHECK(v.N_vertex > 0, "visibility has no vertices");
+  }
+  return v;
+}
+
+Tensor workspace(const Tensor& like, const Common& c, unsigned flags, bool backward) {
+  const size_t bytes = des_shade_workspace_bytes(c.P, c.H, c.W, flags, backward ? 1 : 0, like.get_device());
+  TORCH_CHECK(bytes > 0, "diff_envshade_b200: could not size the workspace");
+  return torch::empty({(int64_t)bytes}, like.options().dtype(torch::kUInt8));
+}
+
+void finish(int st, Tensor& ws, cudaStream_t stream) {
+  raise_status(st);
+  if (check_indices_enabled()) {
+    int status = DES_OK;
+    raise_status(des_workspace_status(ws.data_ptr(), (size_t)ws.numel(), &status,
+                                      reinterpret_cast<des_stream_t>(stream)));
+    raise_status(status);
+  }
+}
+
+const float* fptr(const Tensor& t) { return t.data_ptr<float>(); }
+float* fptr_mut(Tensor& t) { return t.data_ptr<float>(); }
+des_stream_t cur_stream() { return reinterpret_cast<des_stream_t>(at::cuda::getCurrentCUDAStream().stream()); }
+
+// ---------------------------------------------------------------------------------------------
+// Reference surface
+// ---------------------------------------------------------------------------------------------
+
+Tensor bruteforce_diffuse_shader_forward(const Tensor& normal, const Tensor& albedo, const Tensor& envmap,
+                                         const Tensor& R) {
+  Common c = common_checks(normal, albedo, envmap, R);
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  auto opt = normal.options().requires_grad(false);
+  Tensor shading = torch::empty({c.P, c.C}, opt);
+  Tensor ws = workspace(normal, c, DES_DIFFUSE, false);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_bruteforce_diffuse_shader_forward(c.P, c.H, c.W, (int)c.C, fptr(normal), fptr(albedo), fptr(envmap),
+                                                 fptr(R), fptr_mut(shading), ws.data_ptr(), (size_t)ws.numel(),
+                                                 cur_stream());
+  finish(st, ws, stream);
+  return shading;
+}
+
+std::vector<Tensor> bruteforce_diffuse_shader_backward(const Tensor& grad_shading, const Tensor& normal,
+                                                       const Tensor& albedo, const Tensor& envmap, const Tensor& R) {
+  Common c = common_checks(normal, albedo, envmap, R);
+  check_f32(grad_shading, "grad_shading");
+  check_rows(grad_shading, c.P, c.C, "grad_shading");
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  auto opt = normal.options().requires_grad(false);
+  Tensor g_albedo = torch::empty({c.P, c.C}, opt);
+  Tensor g_normal = torch::empty({c.P, 3}, opt);
+  Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
+  Tensor ws = workspace(normal, c, DES_DIFFUSE, true);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_bruteforce_diffuse_shader_backward(c.P, c.H, c.W, (int)c.C, fptr(grad_shading), fptr(normal),
+                                                  fptr(albedo), fptr(envmap), fptr(R), fptr_mut(g_normal),
+                                                  fptr_mut(g_albedo), fptr_mut(g_env), ws.data_ptr(),
+                                                  (size_t)ws.numel(), cur_stream());
+  finish(st, ws, stream);
+  return {g_normal, g_albedo, g_env};
+}
+
+Tensor specular_forward_impl(const Tensor& normal, const Tensor& view, const Tensor& albedo, const Tensor& spec,
+                             const Tensor& rough, const Tensor& envmap, const Tensor& R, bool enable_diffuse,
+                             bool enable_specular, bool clamp) {
+  Common c = common_checks(normal, albedo, envmap, R);
+  spec_checks(c, view, spec, rough);
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  auto opt = normal.options().requires_grad(false);
+  Tensor shading = torch::empty({c.P, c.C}, opt);
+  unsigned f = (enable_diffuse ? DES_DIFFUSE : 0u) | (enable_specular ? DES_SPECULAR : 0u) | (clamp ? DES_CLAMP : 0u);
+  Tensor ws = workspace(normal, c, f, false);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_bruteforce_specular_shader_forward(c.P, c.H, c.W, (int)c.C, fptr(normal), fptr(view), fptr(albedo),
+                                                  fptr(spec), fptr(rough), fptr(envmap), fptr(R), enable_diffuse,
+                                                  enable_specular, clamp, fptr_mut(shading), ws.data_ptr(),
+                                                  (size_t)ws.numel(), cur_stream());
+  finish(st, ws, stream);
+  return shading;
+}
+
+std::vector<Tensor> specular_backward_impl(const Tensor& grad_shading, const Tensor& normal, const Tensor& view,
+                                           const Tensor& albedo, const Tensor& spec, const Tensor& rough,
+                                           const Tensor& envmap, const Tensor& R, bool enable_diffuse,
+                                           bool enable_specular, bool clamp) {
+  Common c = common_checks(normal, albedo, envmap, R);
+  spec_checks(c, view, spec, rough);
+  check_f32(grad_shading, "grad_shading");
+  check_rows(grad_shading, c.P, c.C, "grad_shading");
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  auto opt = normal.options().requires_grad(false);
+  Tensor g_normal = torch::empty({c.P, 3}, opt);
+  Tensor g_view = torch::empty({c.P, 3}, opt);
+  Tensor g_albedo = torch::empty({c.P, c.C}, opt);
+  Tensor g_spec = torch::empty({c.P, c.C}, opt);
+  Tensor g_rough = torch::empty({c.P, 1}, opt);
+  Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
+  unsigned f = (enable_diffuse ? DES_DIFFUSE : 0u) | (enable_specular ? DES_SPECULAR : 0u) | (clamp ? DES_CLAMP : 0u);
+  Tensor ws = workspace(normal, c, f, true);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_bruteforce_specular_shader_backward(
+      c.P, c.H, c.W, (int)c.C, fptr(grad_shading), fptr(normal), fptr(view), fptr(albedo), fptr(spec), fptr(rough),
+      fptr(envmap), fptr(R), enable_diffuse, enable_specular, clamp, fptr_mut(g_normal), fptr_mut(g_view),
+      fptr_mut(g_albedo), fptr_mut(g_spec), fptr_mut(g_rough), fptr_mut(g_env), ws.data_ptr(), (size_t)ws.numel(),
+      cur_stream());
+  finish(st, ws, stream);
+  return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
+}
+
+Tensor bruteforce_specular_shader_forward(const Tensor& normal, const Tensor& view, const Tensor& albedo,
+                                          const Tensor& spec, const Tensor& rough, const Tensor& envmap,
+                                          const Tensor& R, bool enable_diffuse, bool enable_specular) {
+  return specular_forward_impl(normal, view, albedo, spec, rough, envmap, R, enable_diffuse, enable_specular, false);
+}
+std::vector<Tensor> bruteforce_specular_shader_backward(const Tensor& grad_shading, const Tensor& normal,
+                                                        const Tensor& view, const Tensor& albedo,
+                                                        const Tensor& spec, const Tensor& rough,
+                                                        const Tensor& envmap, const Tensor& R, bool enable_diffuse,
+                                                        bool enable_specular) {
+  return specular_backward_impl(grad_shading, normal, view, albedo, spec, rough, envmap, R, enable_diffuse,
+                                enable_specular, false);
+}
+Tensor bruteforce_specular_shader_clamp_forward(const Tensor& normal, const Tensor& view, const Tensor& albedo,
+                                                const Tensor& spec, const Tensor& rough, const Tensor& envmap,
+                                                const Tensor& R, bool enable_diffuse, bool enable_specular) {
+  return specular_forward_impl(normal, view, albedo, spec, rough, envmap, R, enable_diffuse, enable_specular, true);
+}
+std::vector<Tensor> bruteforce_specular_shader_clamp_backward(const Tensor& grad_shading, const Tensor& normal,
+                                                              const Tensor& view, const Tensor& albedo,
+                                                              const Tensor& spec, const Tensor& rough,
+                                                              const Tensor& envmap, const Tensor& R,
+                                                              bool enable_diffuse, bool enable_specular) {
+  return specular_backward_impl(grad_shading, normal, view, albedo, spec, rough, envmap, R, enable_diffuse,
+                                enable_specular, true);
+}
+
+std::vector<Tensor> bruteforce_specular_shader_forward2(const Tensor& normal, const Tensor& view,
+                                                        const Tensor& albedo, const Tensor& spec,
+                                                        const Tensor& rough, const Tensor& envmap, const Tensor& R,
+                                                        bool enable_specular) {
+  Common c = common_checks(normal, albedo, envmap, R);
+  spec_checks(c, view, spec, rough);
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  auto opt = normal.options().requires_grad(false);
+  Tensor shading = torch::empty({c.P, c.C}, opt);
+  Tensor white = torch::empty({c.P, c.C}, opt);
+  unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
+  Tensor ws = workspace(normal, c, f, false);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_bruteforce_specular_shader_forward2(c.P, c.H, c.W, (int)c.C, fptr(normal), fptr(view), fptr(albedo),
+                                                   fptr(spec), fptr(rough), fptr(envmap), fptr(R), enable_specular,
+                                                   fptr_mut(shading), fptr_mut(white), ws.data_ptr(),
+                                                   (size_t)ws.numel(), cur_stream());
+  finish(st, ws, stream);
+  return {shading, white};
+}
+
+std::vector<Tensor> bruteforce_specular_shader_backward2(const Tensor& grad_shading, const Tensor& grad_white,
+                                                         const Tensor& normal, const Tensor& view,
+                                                         const Tensor& albedo, const Tensor& spec,
+                                                         const Tensor& rough, const Tensor& envmap, const Tensor& R,
+                                                         bool enable_specular) {
+  Common c = common_checks(normal, albedo, envmap, R);
+  spec_checks(c, view, spec, rough);
+  check_f32(grad_shading, "grad_shading");
+  check_f32(grad_white, "grad_diffuse_shading");
+  check_rows(grad_shading, c.P, c.C, "grad_shading");
+  check_rows(grad_white, c.P, c.C, "grad_diffuse_shading");
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  auto opt = normal.options().requires_grad(false);
+  Tensor g_normal = torch::empty({c.P, 3}, opt);
+  Tensor g_view = torch::empty({c.P, 3}, opt);
+  Tensor g_albedo = torch::empty({c.P, c.C}, opt);
+  Tensor g_spec = torch::empty({c.P, c.C}, opt);
+  Tensor g_rough = torch::empty({c.P, 1}, opt);
+  Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
+  unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
+  Tensor ws = workspace(normal, c, f, true);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_bruteforce_specular_shader_backward2(
+      c.P, c.H, c.W, (int)c.C, fptr(grad_shading), fptr(grad_white), fptr(normal), fptr(view), fptr(albedo),
+      fptr(spec), fptr(rough), fptr(envmap), fptr(R), enable_specular, fptr_mut(g_normal), fptr_mut(g_view),
+      fptr_mut(g_albedo), fptr_mut(g_spec), fptr_mut(g_rough), fptr_mut(g_env), ws.data_ptr(), (size_t)ws.numel(),
+      cur_stream());
+  finish(st, ws, stream);
+  return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
+}
+
+std::vector<Tensor> bruteforce_specularvisibility_shader_forward2(
+    const Tensor& normal, const Tensor& view, const Tensor& albedo, const Tensor& spec, const Tensor& rough,
+    const Tensor& envmap, const Tensor& R, const Tensor& faces, const Tensor& tri, const Tensor& bary,
+    const Tensor& vis, bool enable_specular) {
+  Common c = common_checks(normal, albedo, envmap, R);
+  spec_checks(c, view, spec, rough);
+  VisArgs v = vis_checks(c, faces, tri, bary, vis);
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  auto opt = normal.options().requires_grad(false);
+  Tensor shading = torch::empty({c.P, c.C}, opt);
+  Tensor white = torch::empty({c.P, c.C}, opt);
+  unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
+  Tensor ws = workspace(normal, c, f, false);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_bruteforce_specularvisibility_shader_forward2(
+      c.P, c.H, c.W, (int)c.C, v.N_face, v.N_vertex, v.N_slot, fptr(normal), fptr(view), fptr(albedo), fptr(spec),
+      fptr(rough), fptr(envmap), fptr(R), faces.data_ptr<int32_t>(), tri.data_ptr<int64_t>(), fptr(bary),
+      vis.data_ptr<int32_t>(), enable_specular, fptr_mut(shading), fptr_mut(white), ws.data_ptr(),
+      (size_t)ws.numel(), cur_stream());
+  finish(st, ws, stream);
+  return {shading, white};
+}
+
+std::vector<Tensor> bruteforce_specularvisibility_shader_backward2(
+    const Tensor& grad_shading, const Tensor& grad_white, const Tensor& normal, const Tensor& view,
+    const Tensor& albedo, const Tensor& spec, const Tensor& rough, const Tensor& envmap, const Tensor& R,
+    const Tensor& faces, const Tensor& tri, const Tensor& bary, const Tensor& vis, bool enable_specular) {
+  Common c = common_checks(normal, albedo, envmap, R);
+  spec_checks(c, view, spec, rough);
+  VisArgs v = vis_checks(c, faces, tri, bary, vis);
+  check_f32(grad_shading, "grad_shading");
+  check_f32(grad_white, "grad_diffuse_shading");
+  check_rows(grad_shading, c.P, c.C, "grad_shading");
+  check_rows(grad_white, c.P, c.C, "grad_diffuse_shading");
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  auto opt = normal.options().requires_grad(false);
+  Tensor g_normal = torch::empty({c.P, 3}, opt);
+  Tensor g_view = torch::empty({c.P, 3}, opt);
+  Tensor g_albedo = torch::empty({c.P, c.C}, opt);
+  Tensor g_spec = torch::empty({c.P, c.C}, opt);
+  Tensor g_rough = torch::empty({c.P, 1}, opt);
+  Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
+  unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
+  Tensor ws = workspace(normal, c, f, true);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_bruteforce_specularvisibility_shader_backward2(
+      c.P, c.H, c.W, (int)c.C, v.N_face, v.N_vertex, v.N_slot, fptr(grad_shading), fptr(grad_white), fptr(normal),
+      fptr(view), fptr(albedo), fptr(spec), fptr(rough), fptr(envmap), fptr(R), faces.data_ptr<int32_t>(),
+      tri.data_ptr<int64_t>(), fptr(bary), vis.data_ptr<int32_t>(), enable_specular, fptr_mut(g_normal),
+      fptr_mut(g_view), fptr_mut(g_albedo), fptr_mut(g_spec), fptr_mut(g_rough), fptr_mut(g_env), ws.data_ptr(),
+      (size_t)ws.numel(), cur_stream());
+  finish(st, ws, stream);
+  return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
+}
+
+// ---------------------------------------------------------------------------------------------
+// Extras (not in the reference)
+// ---------------------------------------------------------------------------------------------
+
+// The rotated texel table the kernels integrate over: [H*W, 4] = (x, y, z, d_omega).
+Tensor texel_table(int64_t H, int64_t W, const Tensor& R) {
+  check_f32(R, "light2obj_rotmat");
+  TORCH_CHECK(R.numel() == 9, "light2obj_rotmat must have 9 elements");
+  const at::cuda::OptionalCUDAGuard guard(device_of(R));
+  Tensor out = torch::empty({H * W, 4}, R.options());
+  raise_status(des_texel_table((int)H, (int)W, fptr(R), fptr_mut(out), cur_stream()));
+  return out;
+}
+
+// Times the main kernel of subsequent shading calls with the caller's CUDA events (raw handles,
+// e.g. torch.cuda.Event().cuda_event); pass 0, 0 to stop.
+void set_timing_events(int64_t start, int64_t stop) {
+  des_set_timing_events(reinterpret_cast<void*>(start), reinterpret_cast<void*>(stop));
+}
+
+int64_t workspace_bytes(int64_t P, int64_t H, int64_t W, int64_t flags, bool backward, int64_t device) {
+  return (int64_t)des_shade_workspace_bytes(P, (int)H, (int)W, (unsigned)flags, backward ? 1 : 0, (int)device);
+}
+
+}  // namespace
+
+PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
+  m.doc() = "B200-native differentiable environment-map shader (reference surface of _diff_envshade)";
+  m.def("bruteforce_diffuse_shader_forward", &bruteforce_diffuse_shader_forward, "bruteforce diffuse shader forward (CUDA)");
+  m.def("bruteforce_diffuse_shader_backward", &bruteforce_diffuse_shader_backward, "bruteforce diffuse shader backward (CUDA)");
+  m.def("bruteforce_specular_shader_forward", &bruteforce_specular_shader_forward, "bruteforce specular shader forward (CUDA)");
+  m.def("bruteforce_specular_shader_backward", &bruteforce_specular_shader_backward, "bruteforce specular shader backward (CUDA)");
+  m.def("bruteforce_specular_shader_clamp_forward", &bruteforce_specular_shader_clamp_forward, "bruteforce specular shader clamp forward (CUDA)");
+  m.def("bruteforce_specular_shader_clamp_backward", &bruteforce_specular_shader_clamp_backward, "bruteforce specular shader clamp backward (CUDA)");
+  m.def("bruteforce_specular_shader_forward2", &bruteforce_specular_shader_forward2, "bruteforce specular shader forward2 (CUDA)");
+  m.def("bruteforce_specular_shader_backward2", &bruteforce_specular_shader_backward2, "bruteforce specular shader backward2 (CUDA)");
+  m.def("bruteforce_specularvisibility_shader_forward2", &bruteforce_specularvisibility_shader_forward2, "bruteforce specular visibility shader forward2 (CUDA)");
+  m.def("bruteforce_specularvisibility_shader_backward2", &bruteforce_specularvisibility_shader_backward2, "bruteforce specular visibility shader backward2 (CUDA)");
+  m.def("texel_table", &texel_table, "rotated texel table [H*W, 4] = (x, y, z, d_omega)");
+  m.def("workspace_bytes", &workspace_bytes, "scratch bytes of one shading call");
+  m.def("set_timing_events", &set_timing_events, "bracket the main kernel of later calls with these CUDA events");
+  m.attr("DES_DIFFUSE") = (int)DES_DIFFUSE;
+  m.attr("DES_SPECULAR") = (int)DES_SPECULAR;
+  m.attr("DES_CLAMP") = (int)DES_CLAMP;
+  m.attr("ABI_VERSION") = des_abi_version();
+}

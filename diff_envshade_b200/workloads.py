@@ -1,0 +1,158 @@
+"""Seeded synthetic shading workloads.
+
+The reference measures on no dataset; these generators produce inputs with the shapes and
+value distributions of the benchmark configurations:
+
+  normals        unit vectors uniform on the sphere (normalised Gaussians)
+  view dirs      unit vectors uniform in the normal's hemisphere (sampled on the sphere, flipped)
+  albedo         U[0,1]^3;  roughness U[r_lo, r_hi];  specular albedo U[0,0.1]^3
+  env map        3 x H x W, radiance exp(N(0, sigma))
+  visibility     each texel bit Bernoulli(p), packed LSB-first, 32 texels per int32 word,
+                 words laid out [N_slot][N_vertex] (texel t -> bit t%32 of slot t//32)
+
+Two visibility layouts exist: ``identity`` (one vertex per point, triangle (p,p,p),
+barycentrics (1,0,0), so each point's visibility is exactly its own bits) and ``mesh``
+(random triangles over P/2 vertices, Dirichlet(1,1,1) barycentrics) which exercises the
+barycentric interpolation.  All draws use a CPU ``torch.Generator`` so the same seed gives the
+same tensors on every machine.
+"""
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+import torch
+
+# name -> (P, H, W, env sigma, roughness range, visibility probability or None, K env maps)
+CONFIGS = {
+    "plain-4k": dict(P=4096, H=16, W=32, sigma=1.0, rough=(0.2, 0.9), vis_p=None, K=1, seed=1234),
+    "vis-70k": dict(P=70000, H=16, W=32, sigma=1.0, rough=(0.2, 0.9), vis_p=0.7, K=1, seed=1235),
+    "vis-1m": dict(P=1048576, H=32, W=64, sigma=1.5, rough=(0.05, 1.0), vis_p=0.6, K=1, seed=1236),
+    "multienv-262k": dict(P=262144, H=16, W=32, sigma=1.0, rough=(0.2, 0.9), vis_p=0.7, K=64, seed=1237),
+}
+
+
+@dataclass
+class ShadeInputs:
+    normal: torch.Tensor
+    view_dir: torch.Tensor
+    albedo: torch.Tensor
+    specular_albedo: torch.Tensor
+    roughness: torch.Tensor
+    envmap: torch.Tensor
+    light2obj_rotmat: torch.Tensor
+    face_vertex_list: Optional[torch.Tensor] = None
+    nearest_triangle_id: Optional[torch.Tensor] = None
+    barycentric_coord: Optional[torch.Tensor] = None
+    visibility: Optional[torch.Tensor] = None
+    grad_shading: Optional[torch.Tensor] = None
+    grad_diffuse_shading: Optional[torch.Tensor] = None
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def P(self):
+        return self.normal.shape[0]
+
+    @property
+    def HW(self):
+        return self.envmap.shape[1] * self.envmap.shape[2]
+
+    @property
+    def has_vis(self):
+        return self.visibility is not None
+
+    def tensors(self):
+        return {k: v for k, v in self.__dict__.items() if isinstance(v, torch.Tensor)}
+
+    def to(self, device):
+        kw = {k: (v.to(device) if isinstance(v, torch.Tensor) else v) for k, v in self.__dict__.items()}
+        return ShadeInputs(**kw)
+
+    def pin(self):
+        kw = {k: (v.pin_memory() if isinstance(v, torch.Tensor) else v) for k, v in self.__dict__.items()}
+        return ShadeInputs(**kw)
+
+    def vis_tuple(self):
+        if not self.has_vis:
+            return None
+        return (self.face_vertex_list, self.nearest_triangle_id, self.barycentric_coord, self.visibility)
+
+
+def _unit(x):
+    return x / x.norm(dim=-1, keepdim=True).clamp_min(1e-12)
+
+
+def random_rotation(g):
+    q = _unit(torch.randn(4, generator=g, dtype=torch.float64))
+    w, x, y, z = q.tolist()
+    R = torch.tensor([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                      [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                      [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]], dtype=torch.float64)
+    return R.float()
+
+
+def pack_bits(bits):
+    """bits: bool [P, n_texels] -> int32 [ceil(n/32), P] words, texel t = bit t%32 of slot t//32."""
+    P, n = bits.shape
+    nslots = (n + 31) // 32
+    b = np.zeros((P, nslots * 32), dtype=np.uint64)
+    b[:, :n] = bits.numpy().astype(np.uint64)
+    b = b.reshape(P, nslots, 32)
+    words = (b << np.arange(32, dtype=np.uint64)).sum(axis=2).astype(np.uint32)  # [P, nslots]
+    return torch.from_numpy(np.ascontiguousarray(words.T).view(np.int32))
+
+
+def unpack_bits(words, n_texels):
+    """int32 [N_slot, N] -> bool [N, n_texels] (inverse of pack_bits)."""
+    w = words.cpu().numpy().view(np.uint32).astype(np.uint64)  # [S, N]
+    bits = ((w[:, None, :] >> np.arange(32, dtype=np.uint64)[None, :, None]) & 1).astype(bool)  # [S, 32, N]
+    bits = bits.reshape(-1, w.shape[1])[:n_texels]
+    return torch.from_numpy(np.ascontiguousarray(bits.T))
+
+
+def make_inputs(P, H, W, seed, sigma=1.0, rough=(0.2, 0.9), vis_p=None, vis_layout="identity", rotation=False,
+                grads=True, env_count=1):
+    g = torch.Generator().manual_seed(seed)
+    n = _unit(torch.randn(P, 3, generator=g))
+    v = _unit(torch.randn(P, 3, generator=g))
+    v = torch.where(((v * n).sum(-1, keepdim=True) < 0), -v, v)
+    albedo = torch.rand(P, 3, generator=g)
+    rough_t = rough[0] + (rough[1] - rough[0]) * torch.rand(P, 1, generator=g)
+    spec = 0.1 * torch.rand(P, 3, generator=g)
+    shape = (3, H, W) if env_count == 1 else (env_count, 3, H, W)
+    env = torch.exp(sigma * torch.randn(*shape, generator=g))
+    R = random_rotation(g) if rotation else torch.eye(3)
+    inp = ShadeInputs(n.contiguous(), v.contiguous(), albedo, spec, rough_t, env.contiguous(), R.contiguous())
+    inp.meta = dict(P=P, H=H, W=W, seed=seed, sigma=sigma, rough=rough, vis_p=vis_p, vis_layout=vis_layout)
+    if vis_p is not None:
+        HW = H * W
+        if vis_layout == "identity":
+            N_vertex = P
+            faces = torch.arange(P, dtype=torch.int32).repeat(3, 1).contiguous()
+            tri = torch.arange(P, dtype=torch.int64)
+            bary = torch.zeros(3, P)
+            bary[0] = 1.0
+        elif vis_layout == "mesh":
+            N_vertex = max(P // 2, 3)
+            N_face = max(P, 1)
+            faces = torch.randint(0, N_vertex, (3, N_face), generator=g, dtype=torch.int64).to(torch.int32)
+            tri = torch.randint(0, N_face, (P,), generator=g, dtype=torch.int64)
+            e = -torch.log(torch.rand(3, P, generator=g).clamp_min(1e-12))
+            bary = (e / e.sum(0, keepdim=True)).contiguous()
+        else:
+            raise ValueError(vis_layout)
+        bits = torch.rand(N_vertex, HW, generator=g) < vis_p
+        inp.face_vertex_list = faces.contiguous()
+        inp.nearest_triangle_id = tri.contiguous()
+        inp.barycentric_coord = bary.contiguous()
+        inp.visibility = pack_bits(bits)
+    if grads:
+        inp.grad_shading = torch.randn(P, 3, generator=g)
+        inp.grad_diffuse_shading = torch.randn(P, 3, generator=g)
+    return inp
+
+
+def make_config(name, **overrides):
+    c = dict(CONFIGS[name])
+    c.update(overrides)
+    return make_inputs(c["P"], c["H"], c["W"], c["seed"], sigma=c["sigma"], rough=c["rough"], vis_p=c["vis_p"],
+                       env_count=c.get("K", 1))

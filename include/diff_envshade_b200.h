@@ -1,0 +1,184 @@
+/*
+ * diff_envshade_b200 -- C ABI of the B200 (sm_100a) environment-map shading kernels.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t, returns a
+ * des_status (0 = DES_OK), launches asynchronously on the given stream, and allocates
+ * nothing: scratch memory is passed in by the caller (size from des_*_workspace_bytes).
+ *
+ * Tensor layouts are the reference extension's (zjumsj/diff_envshade, gsface_shader.h:64-118):
+ *   normal, view_dir, albedo, specular_albedo   P x 3 float32, row-major (AoS)
+ *   roughness                                   P x 1 float32
+ *   envmap                                      C x H x W float32, planar, row 0 = top
+ *   light2obj_rotmat                            3 x 3 float32 row-major, l' = R l
+ *   face_vertex_list                            3 x N_face int32 (SoA)
+ *   nearest_triangle_id                         P int64
+ *   barycentric_coord                           3 x P float32 (SoA)
+ *   visibility                                  N_slot x N_vertex 32-bit words; texel t = row*W + col
+ *                                               is bit (t % 32) of visibility[t / 32][vertex]
+ * Only C == 3 is supported (as in the reference, bruteforce_shader.cu:3332).
+ */
+#ifndef DIFF_ENVSHADE_B200_H_
+#define DIFF_ENVSHADE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* des_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+typedef enum des_status {
+  DES_OK = 0,
+  DES_ERR_INVALID_ARGUMENT = 1, /* a null pointer, negative size, or shapes that do not fit together */
+  DES_ERR_UNSUPPORTED = 2,      /* e.g. C != 3 ("Channel number not supported!") */
+  DES_ERR_WORKSPACE = 3,        /* workspace pointer null, misaligned or too small */
+  DES_ERR_CUDA = 4,             /* a CUDA runtime call or kernel launch failed */
+  DES_ERR_BAD_INDEX = 5,        /* a triangle or vertex id outside its table was seen on the device */
+  DES_ERR_TIMEOUT = 6           /* a bounded device-side wait ran out (serving queue) */
+} des_status;
+
+/* Shading-term switches for des_shade_forward / des_shade_backward. */
+#define DES_DIFFUSE 1u  /* Lambert term                                                 */
+#define DES_SPECULAR 2u /* GGX term (Schlick Fresnel, Schlick-Smith G, GGX NDF)          */
+#define DES_CLAMP 4u    /* backface clamp: a point with n.v <= 0 shades to zero          */
+
+/* All inputs of one shading call.  The visibility block is ignored when visibility == NULL. */
+typedef struct des_shade_args {
+  int64_t P;
+  int32_t H, W, C;
+  const float* normal;
+  const float* view_dir;        /* may be NULL when neither DES_SPECULAR nor DES_CLAMP is set */
+  const float* albedo;          /* may be NULL when DES_DIFFUSE is not set                    */
+  const float* specular_albedo; /* may be NULL when DES_SPECULAR is not set                   */
+  const float* roughness;       /* may be NULL when DES_SPECULAR is not set                   */
+  const float* envmap;
+  const float* light2obj_rotmat;
+  int32_t N_face, N_vertex, N_slot;
+  const int32_t* face_vertex_list;
+  const int64_t* nearest_triangle_id;
+  const float* barycentric_coord;
+  const uint32_t* visibility;   /* NULL = no visibility term */
+} des_shade_args;
+
+/* Human-readable text of a status code (static storage). */
+const char* des_status_string(int status);
+
+/* ABI version of this header (bumped on any signature change). */
+int des_abi_version(void);
+
+/* ---------------------------------------------------------------------------------------
+ * Generic entry points
+ * ------------------------------------------------------------------------------------- */
+
+/* Scratch bytes des_shade_forward (backward = 0) or des_shade_backward (backward = 1) needs for
+ * these sizes on `device`.  Returns 0 on an invalid argument. */
+size_t des_shade_workspace_bytes(int64_t P, int32_t H, int32_t W, unsigned flags, int backward, int device);
+
+/* shading[P x 3] = sum over texels of L * (albedo * diffuse weight + specular_albedo * GGX weight);
+ * diffuse_shading[P x 3] (optional, may be NULL) = the same diffuse sum with a white albedo.
+ * Replaces the kernels behind bruteforce_{diffuse,specular,specular_shader_clamp}_*forward* and
+ * bruteforce_specular{,visibility}_shader_forward2 (reference bruteforce_shader.cu:2687-3336). */
+int des_shade_forward(const des_shade_args* args, unsigned flags, float* shading, float* diffuse_shading,
+                      void* workspace, size_t workspace_bytes, des_stream_t stream);
+
+/* Adjoint of des_shade_forward.  grad_diffuse_shading may be NULL (treated as zero).  Outputs
+ * g_view_dir, g_albedo, g_specular_albedo, g_roughness may be NULL when not wanted; terms that are
+ * switched off produce zeros.  g_envmap[C x H x W] is overwritten (not accumulated); its cross-block
+ * sum runs in FP64 on the device and is deterministic.
+ * Replaces the kernel pairs behind the reference's *_backward / *_backward2 entry points
+ * (bruteforce_shader.cu:2735-2792, 2846-2949, 3002-3106, 3167-3259, 3338-3453). */
+int des_shade_backward(const des_shade_args* args, unsigned flags, const float* grad_shading,
+                       const float* grad_diffuse_shading, float* g_normal, float* g_view_dir, float* g_albedo,
+                       float* g_specular_albedo, float* g_roughness, float* g_envmap, void* workspace,
+                       size_t workspace_bytes, des_stream_t stream);
+
+/* The rotated texel table the kernels integrate over, written to table_out[H*W x 4] as
+ * (x, y, z, d_omega) per texel in memory order.  Bit-exact with the reference's per-pair
+ * getLightDir / getDeltaOmega / rotation (bruteforce_shader.cu:124-147, 2174-2197). */
+int des_texel_table(int32_t H, int32_t W, const float* light2obj_rotmat, float* table_out, des_stream_t stream);
+
+/* Instrumentation.  While both events are set (non-NULL cudaEvent_t handles), every shading call
+ * records `start_event` on its stream immediately before its main kernel (the forward sum or the
+ * fused adjoint) and `stop_event` immediately after it, so the caller can time that kernel alone.
+ * Process-wide; pass NULL, NULL to turn it off. */
+int des_set_timing_events(void* start_event, void* stop_event);
+
+/* Copies the device-side error word of a workspace used by a finished call to *status_out
+ * (DES_OK or DES_ERR_BAD_INDEX) and clears it.  Synchronises `stream`. */
+int des_workspace_status(void* workspace, size_t workspace_bytes, int* status_out, des_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Reference-named entry points: the reference's argument order with tensors as pointers.
+ * Each one replaces the pybind function of the same name (bindings.cpp:6-19).
+ * ------------------------------------------------------------------------------------- */
+
+/* bruteforce_shader.cu:2687 / gsface_shader.h:1 */
+int des_bruteforce_diffuse_shader_forward(int64_t P, int32_t H, int32_t W, int32_t C, const float* normal,
+                                          const float* albedo, const float* envmap, const float* light2obj_rotmat,
+                                          float* shading, void* workspace, size_t workspace_bytes,
+                                          des_stream_t stream);
+/* bruteforce_shader.cu:2735 / gsface_shader.h:8 */
+int des_bruteforce_diffuse_shader_backward(int64_t P, int32_t H, int32_t W, int32_t C, const float* grad_shading,
+                                           const float* normal, const float* albedo, const float* envmap,
+                                           const float* light2obj_rotmat, float* grad_normal, float* grad_albedo,
+                                           float* grad_envmap, void* workspace, size_t workspace_bytes,
+                                           des_stream_t stream);
+/* bruteforce_shader.cu:2796 (clamp = 0) and 2953 (clamp = 1) / gsface_shader.h:16, 40 */
+int des_bruteforce_specular_shader_forward(int64_t P, int32_t H, int32_t W, int32_t C, const float* normal,
+                                           const float* view_dir, const float* albedo,
+                                           const float* specular_albedo, const float* roughness,
+                                           const float* envmap, const float* light2obj_rotmat, int enable_diffuse,
+                                           int enable_specular, int clamp, float* shading, void* workspace,
+                                           size_t workspace_bytes, des_stream_t stream);
+/* bruteforce_shader.cu:2846 (clamp = 0) and 3002 (clamp = 1) / gsface_shader.h:27, 51 */
+int des_bruteforce_specular_shader_backward(int64_t P, int32_t H, int32_t W, int32_t C, const float* grad_shading,
+                                            const float* normal, const float* view_dir, const float* albedo,
+                                            const float* specular_albedo, const float* roughness,
+                                            const float* envmap, const float* light2obj_rotmat,
+                                            int enable_diffuse, int enable_specular, int clamp,
+                                            float* grad_normal, float* grad_view_dir, float* grad_albedo,
+                                            float* grad_specular_albedo, float* grad_roughness,
+                                            float* grad_envmap, void* workspace, size_t workspace_bytes,
+                                            des_stream_t stream);
+/* bruteforce_shader.cu:3108 / gsface_shader.h:64 */
+int des_bruteforce_specular_shader_forward2(int64_t P, int32_t H, int32_t W, int32_t C, const float* normal,
+                                            const float* view_dir, const float* albedo,
+                                            const float* specular_albedo, const float* roughness,
+                                            const float* envmap, const float* light2obj_rotmat,
+                                            int enable_specular, float* shading, float* diffuse_shading,
+                                            void* workspace, size_t workspace_bytes, des_stream_t stream);
+/* bruteforce_shader.cu:3167 / gsface_shader.h:75 */
+int des_bruteforce_specular_shader_backward2(int64_t P, int32_t H, int32_t W, int32_t C,
+                                             const float* grad_shading, const float* grad_diffuse_shading,
+                                             const float* normal, const float* view_dir, const float* albedo,
+                                             const float* specular_albedo, const float* roughness,
+                                             const float* envmap, const float* light2obj_rotmat,
+                                             int enable_specular, float* grad_normal, float* grad_view_dir,
+                                             float* grad_albedo, float* grad_specular_albedo,
+                                             float* grad_roughness, float* grad_envmap, void* workspace,
+                                             size_t workspace_bytes, des_stream_t stream);
+/* bruteforce_shader.cu:3261 / gsface_shader.h:88 */
+int des_bruteforce_specularvisibility_shader_forward2(
+    int64_t P, int32_t H, int32_t W, int32_t C, int32_t N_face, int32_t N_vertex, int32_t N_slot,
+    const float* normal, const float* view_dir, const float* albedo, const float* specular_albedo,
+    const float* roughness, const float* envmap, const float* light2obj_rotmat, const int32_t* face_vertex_list,
+    const int64_t* nearest_triangle_id, const float* barycentric_coord, const int32_t* visibility,
+    int enable_specular, float* shading, float* diffuse_shading, void* workspace, size_t workspace_bytes,
+    des_stream_t stream);
+/* bruteforce_shader.cu:3338 / gsface_shader.h:103 */
+int des_bruteforce_specularvisibility_shader_backward2(
+    int64_t P, int32_t H, int32_t W, int32_t C, int32_t N_face, int32_t N_vertex, int32_t N_slot,
+    const float* grad_shading, const float* grad_diffuse_shading, const float* normal, const float* view_dir,
+    const float* albedo, const float* specular_albedo, const float* roughness, const float* envmap,
+    const float* light2obj_rotmat, const int32_t* face_vertex_list, const int64_t* nearest_triangle_id,
+    const float* barycentric_coord, const int32_t* visibility, int enable_specular, float* grad_normal,
+    float* grad_view_dir, float* grad_albedo, float* grad_specular_albedo, float* grad_roughness,
+    float* grad_envmap, void* workspace, size_t workspace_bytes, des_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIFF_ENVSHADE_B200_H_ */

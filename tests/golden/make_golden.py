@@ -1,0 +1,151 @@
+"""Generate the golden fixtures of the shading path from the reference extension.
+
+Runs on a CUDA machine with the reference extension built by ``oracle/build_ref.py``
+(``oracle/_ref/_diff_envshade*.so``) and this package built.  For each case it draws seeded
+inputs, runs the reference operator, and stores inputs + reference outputs in
+``<out>/<case>.npz``; the texel table this package computes (``texel_table``) is stored
+beside them so the CPU oracle can be checked against the reference without a GPU.
+
+It also writes ``table_probe_<H>x<W>.npz``: the reference's white-diffuse output for points
+that each see exactly one texel through a one-hot visibility word, with axis-aligned normals
+and unit radiance.  That output equals fl(fl(+-l_k / pi) * d_omega) for the texel's rotated
+direction component l_k, which pins the texel table bit-for-bit.
+
+Usage:  python tests/golden/make_golden.py --out tests/golden
+"""
+import argparse
+import glob
+import os
+import sys
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+
+def load_reference():
+    refdir = os.path.join(ROOT, "oracle", "_ref")
+    if not glob.glob(os.path.join(refdir, "_diff_envshade*.so")):
+        raise SystemExit("reference extension not built (python oracle/build_ref.py)")
+    sys.path.insert(0, refdir)
+    import _diff_envshade  # noqa: E402
+    return _diff_envshade
+
+
+# case name -> (op, P, H, W, seed, vis layout or None, enable_diffuse, enable_specular, rotation, rough range)
+CASES = {
+    "vis2_mesh_16x32": ("specularvisibility2", 256, 16, 32, 11, "mesh", True, True, True, (0.2, 0.9)),
+    "vis2_identity_16x32": ("specularvisibility2", 256, 16, 32, 12, "identity", True, True, False, (0.2, 0.9)),
+    "vis2_mesh_ragged_5x7_nospec": ("specularvisibility2", 200, 5, 7, 13, "mesh", True, False, True, (0.2, 0.9)),
+    "vis2_mesh_32x64_rough": ("specularvisibility2", 128, 32, 64, 14, "mesh", True, True, True, (0.05, 1.0)),
+    "spec2_16x32": ("specular2", 256, 16, 32, 21, None, True, True, True, (0.2, 0.9)),
+    "spec2_16x32_nospec": ("specular2", 256, 16, 32, 22, None, True, False, False, (0.2, 0.9)),
+    "spec2_ragged_9x13": ("specular2", 100, 9, 13, 23, None, True, True, True, (0.2, 0.9)),
+    "spec_v1_16x32": ("specular", 256, 16, 32, 31, None, True, True, True, (0.2, 0.9)),
+    "spec_v1_specular_only": ("specular", 256, 16, 32, 32, None, False, True, False, (0.2, 0.9)),
+    "spec_v1_diffuse_only": ("specular", 256, 16, 32, 33, None, True, False, True, (0.2, 0.9)),
+    "clamp_16x32": ("specular_clamp", 256, 16, 32, 41, None, True, True, True, (0.2, 0.9)),
+    "clamp_16x32_diffuse_only": ("specular_clamp", 256, 16, 32, 42, None, True, False, False, (0.2, 0.9)),
+    "diffuse_16x32": ("diffuse", 256, 16, 32, 51, None, True, False, True, (0.2, 0.9)),
+}
+
+
+def run_reference(ref, op, inp, ed, es):
+    d = {k: v.cuda() for k, v in inp.tensors().items()}
+    n, v, a, s, r, env, R = (d["normal"], d["view_dir"], d["albedo"], d["specular_albedo"], d["roughness"],
+                             d["envmap"], d["light2obj_rotmat"])
+    gs, gw = d["grad_shading"], d["grad_diffuse_shading"]
+    out = {}
+    if op == "specularvisibility2":
+        vis = (d["face_vertex_list"], d["nearest_triangle_id"], d["barycentric_coord"], d["visibility"])
+        sh, wh = ref.bruteforce_specularvisibility_shader_forward2(n, v, a, s, r, env, R, *vis, es)
+        g = ref.bruteforce_specularvisibility_shader_backward2(gs, gw, n, v, a, s, r, env, R, *vis, es)
+        out.update(shading=sh, diffuse_shading=wh)
+    elif op == "specular2":
+        sh, wh = ref.bruteforce_specular_shader_forward2(n, v, a, s, r, env, R, es)
+        g = ref.bruteforce_specular_shader_backward2(gs, gw, n, v, a, s, r, env, R, es)
+        out.update(shading=sh, diffuse_shading=wh)
+    elif op == "specular":
+        sh = ref.bruteforce_specular_shader_forward(n, v, a, s, r, env, R, ed, es)
+        g = ref.bruteforce_specular_shader_backward(gs, n, v, a, s, r, env, R, ed, es)
+        out.update(shading=sh)
+    elif op == "specular_clamp":
+        sh = ref.bruteforce_specular_shader_clamp_forward(n, v, a, s, r, env, R, ed, es)
+        g = ref.bruteforce_specular_shader_clamp_backward(gs, n, v, a, s, r, env, R, ed, es)
+        out.update(shading=sh)
+    elif op == "diffuse":
+        sh = ref.bruteforce_diffuse_shader_forward(n, a, env, R)
+        gn, ga, ge = ref.bruteforce_diffuse_shader_backward(gs, n, a, env, R)
+        g = [gn, None, ga, None, None, ge]
+        out.update(shading=sh)
+    else:
+        raise ValueError(op)
+    names = ["g_normal", "g_view", "g_albedo", "g_spec", "g_rough", "g_env"]
+    for k, t in zip(names, g):
+        if t is not None:
+            out[k] = t
+    torch.cuda.synchronize()
+    return {k: t.detach().cpu().numpy() for k, t in out.items()}
+
+
+def table_probe_inputs(H, W, R):
+    """P = 6*H*W points: point (t, k) has normal +-e_axis, one-hot visibility on texel t."""
+    HW = H * W
+    axes = torch.tensor([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], dtype=torch.float32)
+    P = 6 * HW
+    normal = axes.repeat(HW, 1).contiguous()                    # point index = t*6 + k
+    texel = torch.arange(HW).repeat_interleave(6)
+    nslots = (HW + 31) // 32
+    w = np.zeros((nslots, P), dtype=np.uint32)
+    t = texel.numpy()
+    w[t // 32, np.arange(P)] = (np.uint32(1) << (t % 32).astype(np.uint32))
+    words = torch.from_numpy(w.view(np.int32))
+    return dict(
+        normal=normal, view_dir=normal.clone(), albedo=torch.ones(P, 3), specular_albedo=torch.zeros(P, 3),
+        roughness=torch.full((P, 1), 0.5), envmap=torch.ones(3, H, W), light2obj_rotmat=R.float().contiguous(),
+        face_vertex_list=torch.arange(P, dtype=torch.int32).repeat(3, 1).contiguous(),
+        nearest_triangle_id=torch.arange(P, dtype=torch.int64),
+        barycentric_coord=torch.cat([torch.ones(1, P), torch.zeros(2, P)]).contiguous(),
+        visibility=words.contiguous())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    ref = load_reference()
+    import diff_envshade_b200 as des
+    from diff_envshade_b200 import workloads as wl
+
+    for name, (op, P, H, W, seed, layout, ed, es, rot, rough) in CASES.items():
+        inp = wl.make_inputs(P, H, W, seed, rough=rough, vis_p=(0.7 if layout else None),
+                             vis_layout=(layout or "identity"), rotation=rot)
+        outs = run_reference(ref, op, inp, ed, es)
+        table = des.texel_table(H, W, inp.light2obj_rotmat.cuda()).cpu().numpy()
+        arrays = {f"in_{k}": v.numpy() for k, v in inp.tensors().items()}
+        arrays.update({f"ref_{k}": v for k, v in outs.items()})
+        arrays["table"] = table
+        meta = np.array([op, str(P), str(H), str(W), str(seed), str(layout), str(int(ed)), str(int(es))])
+        np.savez_compressed(os.path.join(a.out, f"{name}.npz"), meta=meta, **arrays)
+        print("wrote", name, {k: v.shape for k, v in outs.items()})
+
+    g = torch.Generator().manual_seed(99)
+    for (H, W, rot) in [(16, 32, False), (32, 64, False), (7, 9, True), (16, 32, True)]:
+        R = wl.random_rotation(g) if rot else torch.eye(3)
+        d = {k: v.cuda() for k, v in table_probe_inputs(H, W, R).items()}
+        _, white = ref.bruteforce_specularvisibility_shader_forward2(
+            d["normal"], d["view_dir"], d["albedo"], d["specular_albedo"], d["roughness"], d["envmap"],
+            d["light2obj_rotmat"], d["face_vertex_list"], d["nearest_triangle_id"], d["barycentric_coord"],
+            d["visibility"], False)
+        table = des.texel_table(H, W, d["light2obj_rotmat"]).cpu().numpy()
+        tag = f"{H}x{W}" + ("_rot" if rot else "")
+        np.savez_compressed(os.path.join(a.out, f"table_probe_{tag}.npz"), R=R.numpy(),
+                            ref_white=white[:, 0].cpu().numpy(), table=table)
+        print("wrote table probe", tag)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+"""CPU tests of the oracle: self-consistency, finite differences, and the golden vectors the
+reference extension produced (tests/golden/*.npz, made by tests/golden/make_golden.py)."""
+import copy
+import os
+
+import numpy as np
+import pytest
+
+from conftest import assert_close_fwd, assert_close_grad, golden_files
+from oracle import oracle as orc
+from diff_envshade_b200 import workloads as wl
+
+OPS = [
+    ("diffuse", True, False),
+    ("specular", True, True),
+    ("specular", False, True),
+    ("specular_clamp", True, True),
+    ("specular2", True, True),
+    ("specular2", True, False),
+    ("specularvisibility2", True, True),
+]
+
+
+def _loss(inp, flags, table, gs, gw):
+    sh, wh = orc.forward(inp, flags, table=table)
+    return float((gs * sh).sum() + (gw * wh).sum())
+
+
+@pytest.mark.parametrize("op,ed,es", OPS)
+def test_oracle_backward_matches_central_differences(op, ed, es):
+    """The restated adjoint (bruteforce_shader.cu:149-227, 1701-2683) is the gradient of the
+    restated forward: central differences in FP64, h = 1e-6, on 6 points."""
+    vis = op == "specularvisibility2"
+    inp = wl.make_inputs(6, 8, 16, seed=7, vis_p=0.7 if vis else None, vis_layout="mesh", rotation=True)
+    flags = orc.flags_for(op, ed, es)
+    table = orc.texel_table_f64(8, 16, inp.light2obj_rotmat)
+    gs = inp.grad_shading.double().numpy()
+    gw = inp.grad_diffuse_shading.double().numpy() if flags & orc.WHITE else np.zeros_like(gs)
+    out = orc.backward(inp, flags, gs, gw if flags & orc.WHITE else None, table=table)
+    h = 1e-6
+    for name, key in [("normal", "g_normal"), ("view_dir", "g_view"), ("albedo", "g_albedo"),
+                      ("specular_albedo", "g_spec"), ("roughness", "g_rough")]:
+        base = getattr(inp, name).double().numpy()
+        num = np.zeros_like(base)
+        for i in range(base.shape[0]):
+            for j in range(base.shape[1]):
+                for sgn in (1, -1):
+                    x = base.copy()
+                    x[i, j] += sgn * h
+                    i2 = copy.copy(inp)
+                    setattr(i2, name, x)
+                    num[i, j] += sgn * _loss(i2, flags, table, gs, gw) / (2 * h)
+        ana = out[key]
+        scale = max(np.abs(num).max(), np.abs(ana).max(), 1e-12)
+        assert np.abs(num - ana).max() / scale < 1e-6, (op, name, num, ana)
+    # env map: the loss is linear in it, so the difference quotient is exact up to rounding
+    env = inp.envmap.double().numpy()
+    for (c, y, x) in [(0, 0, 0), (1, 3, 7), (2, 7, 15)]:
+        vals = []
+        for sgn in (1, -1):
+            e = env.copy()
+            e[c, y, x] += sgn * 1e-3
+            i2 = copy.copy(inp)
+            i2.envmap = e
+            vals.append(_loss(i2, flags, table, gs, gw))
+        num = (vals[0] - vals[1]) / 2e-3
+        assert abs(num - out["g_env"][c, y, x]) <= 1e-8 * max(1.0, abs(num)), (op, c, y, x)
+
+
+def test_texel_table_solid_angles_cover_the_sphere():
+    for H, W in [(16, 32), (32, 64), (5, 7)]:
+        t = orc.texel_table_f64(H, W)
+        assert abs(t[:, 3].sum() - 4 * np.pi) < 1e-9
+        assert np.allclose(np.linalg.norm(t[:, :3], axis=1), 1.0)
+        # memory row 0 is the top row (+y), LEFT_TOP_AS_ORIGIN
+        assert t[0, 1] > 0 and t[-1, 1] < 0
+
+
+def test_constant_radiance_diffuse_integrates_to_one():
+    """With L = 1 and albedo 1 the white diffuse output approximates int max(n.l,0)/pi = 1."""
+    inp = wl.make_inputs(64, 64, 128, seed=3)
+    inp.envmap = np.ones((3, 64, 128))
+    sh, wh = orc.forward(inp, orc.flags_for("specular2", True, False))
+    assert np.abs(wh - 1.0).max() < 2e-3
+
+
+def test_fp32_oracle_tracks_fp64():
+    inp = wl.make_inputs(128, 16, 32, seed=5, vis_p=0.7, vis_layout="mesh", rotation=True)
+    f = orc.flags_for("specularvisibility2")
+    table = orc.texel_table_f64(16, 32, inp.light2obj_rotmat).astype(np.float32)
+    s64, w64 = orc.forward(inp, f, table=table)
+    s32, w32 = orc.forward(inp, f, table=table, dtype=np.float32)
+    assert_close_fwd(s32, s64, "shading f32", rtol=2e-5)
+    assert_close_fwd(w32, w64, "white f32", rtol=2e-5)
+    gs, gw = inp.grad_shading.numpy(), inp.grad_diffuse_shading.numpy()
+    b64 = orc.backward(inp, f, gs, gw, table=table)
+    b32 = orc.backward(inp, f, gs, gw, table=table, dtype=np.float32)
+    for k in b64:
+        assert_close_grad(b32[k], b64[k], k, rtol=3e-4)
+
+
+def test_oracle_deterministic_across_thread_counts():
+    inp = wl.make_inputs(97, 16, 32, seed=9, vis_p=0.6, vis_layout="mesh")
+    f = orc.flags_for("specularvisibility2")
+    gs, gw = inp.grad_shading.numpy(), inp.grad_diffuse_shading.numpy()
+    a = orc.backward(inp, f, gs, gw, nthreads=1)
+    b = orc.backward(inp, f, gs, gw, nthreads=7)
+    for k in a:
+        np.testing.assert_allclose(a[k], b[k], rtol=1e-12, atol=1e-14)
+
+
+def test_visibility_pack_roundtrip_and_bit_order():
+    import torch
+    g = torch.Generator().manual_seed(0)
+    bits = torch.rand(37, 75, generator=g) < 0.5
+    words = wl.pack_bits(bits)
+    assert words.shape == (3, 37) and words.dtype == torch.int32
+    assert torch.equal(wl.unpack_bits(words, 75), bits)
+    one = torch.zeros(1, 64, dtype=torch.bool)
+    one[0, 37] = True
+    w = wl.pack_bits(one).numpy().view(np.uint32)
+    assert w[1, 0] == 1 << 5 and w[0, 0] == 0
+
+
+def test_identity_visibility_masks_texels():
+    """Identity layout: each point's visibility is exactly its bits; all-ones bits = no visibility."""
+    inp = wl.make_inputs(40, 8, 16, seed=21, vis_p=1.0)
+    f_vis = orc.flags_for("specularvisibility2")
+    f_plain = orc.flags_for("specular2")
+    a = orc.forward(inp, f_vis)
+    inp2 = copy.copy(inp)
+    inp2.visibility = None
+    b = orc.forward(inp2, f_plain)
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-12)
+    np.testing.assert_allclose(a[1], b[1], rtol=1e-12)
+
+
+CASES = golden_files("[!t]*.npz")
+
+
+@pytest.mark.skipif(not CASES, reason="golden fixtures not generated")
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p)[:-4] for p in CASES])
+def test_oracle_against_reference_golden(path):
+    """The FP64 oracle, given the GPU texel table, reproduces the reference extension's outputs
+    (forward rel 1e-5, gradients rel 1e-4 of the tensor scale)."""
+    z = np.load(path)
+    op, P, H, W, seed, layout, ed, es = z["meta"]
+    ed, es = bool(int(ed)), bool(int(es))
+    inp = wl.ShadeInputs(*(z[f"in_{k}"] for k in ("normal", "view_dir", "albedo", "specular_albedo", "roughness",
+                                                  "envmap", "light2obj_rotmat")))
+    if "in_visibility" in z:
+        inp.face_vertex_list = z["in_face_vertex_list"]
+        inp.nearest_triangle_id = z["in_nearest_triangle_id"]
+        inp.barycentric_coord = z["in_barycentric_coord"]
+        inp.visibility = z["in_visibility"]
+    flags = orc.flags_for(op, ed, es)
+    table = z["table"]
+    sh, wh = orc.forward(inp, flags, table=table)
+    assert_close_fwd(sh, z["ref_shading"], "shading")
+    if "ref_diffuse_shading" in z:
+        assert_close_fwd(wh, z["ref_diffuse_shading"], "diffuse_shading")
+    gw = z["in_grad_diffuse_shading"] if flags & orc.WHITE else None
+    out = orc.backward(inp, flags, z["in_grad_shading"], gw, table=table)
+    for k in ("g_normal", "g_view", "g_albedo", "g_spec", "g_rough", "g_env"):
+        if f"ref_{k}" in z:
+            assert_close_grad(out[k], z[f"ref_{k}"], k)
