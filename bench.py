@@ -230,6 +230,10 @@ def main():
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     kf = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     kb = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    for pair in kf + kb:  # torch creates events lazily: record once so the raw handles exist
+        for e in pair:
+            e.record()
+    torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
     if pg is not None:

@@ -36,6 +36,7 @@ from ._C import (  # noqa: E402,F401  reference operator surface
     bruteforce_specularvisibility_shader_backward2,
     texel_table,
     workspace_bytes,
+    set_timing_events,
 )
 from .autograd import (  # noqa: E402,F401
     DiffuseShade,

@@ -46,12 +46,16 @@ __device__ __forceinline__ float3 texel_direction(int iy, int ix, int W, int H) 
   return c;
 }
 
-// l' = R l with the reference's expression order (bruteforce_shader.cu:2194-2197).
+// l' = R l (bruteforce_shader.cu:2194-2197).  The reference writes each row as
+// m0*x + m1*y + m2*z and leaves the FMA contraction to nvcc; its compiled kernels evaluate row 0 as
+// fma(m2, z, fma(m1, y, m0*x)) and rows 1 and 2 as fma(m5, z, fma(m3, x, m4*y)).  That order was
+// identified from the reference's own outputs (tests/golden/table_probe_*) and is spelled out here
+// with explicit round-to-nearest intrinsics, so the table does not depend on contraction choices.
 __device__ __forceinline__ float3 rotate3(const float* m, float3 l) {
   float3 r;
-  r.x = m[0] * l.x + m[1] * l.y + m[2] * l.z;
-  r.y = m[3] * l.x + m[4] * l.y + m[5] * l.z;
-  r.z = m[6] * l.x + m[7] * l.y + m[8] * l.z;
+  r.x = __fmaf_rn(m[2], l.z, __fmaf_rn(m[1], l.y, __fmul_rn(m[0], l.x)));
+  r.y = __fmaf_rn(m[5], l.z, __fmaf_rn(m[3], l.x, __fmul_rn(m[4], l.y)));
+  r.z = __fmaf_rn(m[8], l.z, __fmaf_rn(m[6], l.x, __fmul_rn(m[7], l.y)));
   return r;
 }
 

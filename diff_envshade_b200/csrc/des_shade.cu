@@ -155,6 +155,7 @@ struct SpecConst {
   float k, omk;       // k = (r+1)^2/8 and 1 - k
   float invB;         // 1 / (max(n.v,0) (1-k) + k)
   float nvp;          // max(n.v, 0)
+  float omn;          // 1 - |n|^2 (zero for an exactly unit normal)
 };
 
 __device__ __forceinline__ SpecConst spec_const(float r, const PointGeom& g) {
@@ -167,7 +168,21 @@ __device__ __forceinline__ SpecConst spec_const(float r, const PointGeom& g) {
   s.omk = 1.f - s.k;
   s.nvp = fmaxf(dot3(g.vx, g.vy, g.vz, g.nx, g.ny, g.nz), 0.f);
   s.invB = 1.f / fmaf(s.nvp, s.omk, s.k);
+  const double n2 = (double)g.nx * g.nx + (double)g.ny * g.ny + (double)g.nz * g.nz;
+  s.omn = (float)(1.0 - n2);
   return s;
+}
+
+// GGX denominator t = (n.h)^2 (alpha^2 - 1) + 1 for h = h0 / |h0|, evaluated without cancellation:
+// 1 - (n.h)^2 = |n x h0|^2 / |h0|^2 + (1 - |n|^2), so t = |n x h0|^2 ri2 + omn + (n.h)^2 alpha^2.
+// Near the specular peak t ~ alpha^2 << 1, where the direct form loses ~log2(1/alpha^2) bits.
+__device__ __forceinline__ float ggx_t(const PointGeom& g, float hx, float hy, float hz, float ri, float nh2,
+                                       const SpecConst& sc) {
+  const float cx = fmaf(g.ny, hz, -g.nz * hy);
+  const float cy = fmaf(g.nz, hx, -g.nx * hz);
+  const float cz = fmaf(g.nx, hy, -g.ny * hx);
+  const float cc = dot3(cx, cy, cz, cx, cy, cz);
+  return fmaf(nh2, sc.alpha2, fmaf(cc, ri * ri, sc.omn));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -251,7 +266,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_fwd_kernel(const ShadePara
               const float a2 = a * a;
               const float F = fmaf(a2 * a2 * a, 1.f - kR0, kR0);
               const float G = nl * rcp_approx(fmaf(nl, sc.omk, sc.k)) * sc.invB;
-              const float tt = fmaf(nh * nh, sc.am1, 1.f);
+              const float tt = ggx_t(g, hx, hy, hz, ri, nh * nh, sc);
               const float D = sc.alpha2 * rcp_approx(fmaxf(kPiF * tt * tt, kThres));
               const float tmp = F * G * D * 0.25f;
               const float ws = (act && tmp > 0.f) ? tmp * A.w * vis : 0.f;
@@ -449,7 +464,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
               const float Ga = nl * ia;
               const float G = Ga * sc.invB;
               const float nh2 = nh * nh;
-              const float tt = fmaf(nh2, sc.am1, 1.f);
+              const float tt = ggx_t(g, hx, hy, hz, ri, nh2, sc);
               const float t2 = kPiF * tt * tt;
               const float itm = rcp_approx(fmaxf(t2, kThres));
               const float D = sc.alpha2 * itm;

@@ -49,7 +49,9 @@ def err_stats(got, ref):
     return float(d.max() / scale) if d.size else 0.0, d, scale
 
 
-def assert_close_fwd(got, ref, name="", rtol=FWD_RTOL, floor=FWD_FLOOR):
+def assert_close_fwd(got, ref, name="", rtol=FWD_RTOL, floor=FWD_FLOOR, allowance=None):
+    """Per element |got - ref| <= rtol (|ref| + floor max|ref|) + allowance (an optional per-element
+    array: the reference's own measured deviation from exact arithmetic)."""
     g, r = _np(got), _np(ref)
     assert g.shape == r.shape, (name, g.shape, r.shape)
     if r.size == 0:
@@ -57,13 +59,17 @@ def assert_close_fwd(got, ref, name="", rtol=FWD_RTOL, floor=FWD_FLOOR):
     assert np.isfinite(g).all(), f"{name}: non-finite values"
     scale = max(np.abs(r).max(), 1e-30)
     bound = rtol * np.abs(r) + rtol * floor * scale
+    if allowance is not None:
+        bound = bound + _np(allowance)
     d = np.abs(g - r)
     worst = np.argmax(d - bound)
     assert (d <= bound).all(), (f"{name}: max rel err {np.max(d / (np.abs(r) + floor * scale)):.3e} "
                                 f"at {np.unravel_index(worst, d.shape)} got {g.flat[worst]!r} ref {r.flat[worst]!r}")
 
 
-def assert_close_grad(got, ref, name="", rtol=GRAD_RTOL, floor=GRAD_FLOOR):
+def assert_close_grad(got, ref, name="", rtol=GRAD_RTOL, floor=GRAD_FLOOR, allowance=None):
+    """Per tensor max|got - ref| / max|ref| <= rtol and per element
+    |got - ref| <= rtol (|ref| + floor max|ref|), both widened by an optional per-element allowance."""
     g, r = _np(got), _np(ref)
     assert g.shape == r.shape, (name, g.shape, r.shape)
     if r.size == 0:
@@ -73,9 +79,10 @@ def assert_close_grad(got, ref, name="", rtol=GRAD_RTOL, floor=GRAD_FLOOR):
     if scale == 0:
         assert np.abs(g).max() == 0, f"{name}: expected zeros"
         return
+    allow = np.zeros_like(r) if allowance is None else _np(allowance)
     d = np.abs(g - r)
-    assert d.max() / scale <= rtol, f"{name}: tensor rel err {d.max() / scale:.3e}"
-    bound = rtol * np.abs(r) + rtol * floor * scale
+    assert (d - allow).max() / scale <= rtol, f"{name}: tensor rel err {d.max() / scale:.3e}"
+    bound = rtol * np.abs(r) + rtol * floor * scale + allow
     worst = np.argmax(d - bound)
     assert (d <= bound).all(), (f"{name}: element err {d.flat[worst]:.3e} vs bound {bound.flat[worst]:.3e} "
                                 f"(ref {r.flat[worst]!r})")

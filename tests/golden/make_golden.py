@@ -135,16 +135,69 @@ def main():
     g = torch.Generator().manual_seed(99)
     for (H, W, rot) in [(16, 32, False), (32, 64, False), (7, 9, True), (16, 32, True)]:
         R = wl.random_rotation(g) if rot else torch.eye(3)
-        d = {k: v.cuda() for k, v in table_probe_inputs(H, W, R).items()}
-        _, white = ref.bruteforce_specularvisibility_shader_forward2(
-            d["normal"], d["view_dir"], d["albedo"], d["specular_albedo"], d["roughness"], d["envmap"],
-            d["light2obj_rotmat"], d["face_vertex_list"], d["nearest_triangle_id"], d["barycentric_coord"],
-            d["visibility"], False)
-        table = des.texel_table(H, W, d["light2obj_rotmat"]).cpu().numpy()
         tag = f"{H}x{W}" + ("_rot" if rot else "")
-        np.savez_compressed(os.path.join(a.out, f"table_probe_{tag}.npz"), R=R.numpy(),
-                            ref_white=white[:, 0].cpu().numpy(), table=table)
-        print("wrote table probe", tag)
+        arrays = table_probes(ref, H, W, R, one_hot_env=(H * W <= 512))
+        arrays["table"] = des.texel_table(H, W, R.float().cuda()).cpu().numpy()
+        arrays["R"] = R.numpy()
+        np.savez_compressed(os.path.join(a.out, f"table_probe_{tag}.npz"), **arrays)
+        print("wrote table probe", tag, sorted(arrays))
+
+
+def table_probes(ref, H, W, R, one_hot_env):
+    """Reference outputs that each reduce to fl(fl(+-l_axis / pi) * d_omega) for single texels.
+
+    ref_white        Forward2 with visibility: point (t, axis) sees only texel t       [6*HW]
+    ref_galbedo      Backward2 with visibility, grad_shading = 1: its g_albedo          [6*HW]
+    ref_genv         BackwardEnvmap2 with visibility, one axis per call, grad_diffuse = 1 [6, HW]
+    ref_white_novis  Forward2 without visibility, one-hot env map per call (small maps) [HW, 6]
+    ref_genv_novis   BackwardEnvmap2 without visibility, 6 axis points, grad_diffuse = 1 [HW]
+                     (the sum over the positive-cosine points, in point order)
+    """
+    HW = H * W
+    out = {}
+    d = {k: v.cuda() for k, v in table_probe_inputs(H, W, R).items()}
+    vis = (d["face_vertex_list"], d["nearest_triangle_id"], d["barycentric_coord"], d["visibility"])
+    base = (d["normal"], d["view_dir"], d["albedo"], d["specular_albedo"], d["roughness"], d["envmap"],
+            d["light2obj_rotmat"])
+    _, white = ref.bruteforce_specularvisibility_shader_forward2(*base, *vis, False)
+    out["ref_white"] = white[:, 0].cpu().numpy()
+    ones = torch.ones_like(d["normal"])
+    g = ref.bruteforce_specularvisibility_shader_backward2(ones, torch.zeros_like(ones), *base, *vis, False)
+    out["ref_galbedo"] = g[2][:, 0].cpu().numpy()
+    genv = []
+    for k in range(6):
+        sel = torch.arange(k, 6 * HW, 6, device="cuda")  # point t*6+k: texel t, axis k
+        sub = {n: d[n][sel].contiguous() for n in ("normal", "view_dir", "albedo", "specular_albedo", "roughness")}
+        P = HW
+        faces = torch.arange(P, dtype=torch.int32, device="cuda").repeat(3, 1).contiguous()
+        tri = torch.arange(P, dtype=torch.int64, device="cuda")
+        bary = torch.cat([torch.ones(1, P), torch.zeros(2, P)]).cuda().contiguous()
+        bits = d["visibility"][:, sel].contiguous()
+        zeros = torch.zeros(P, 3, device="cuda")
+        gk = ref.bruteforce_specularvisibility_shader_backward2(
+            zeros, torch.ones(P, 3, device="cuda"), sub["normal"], sub["view_dir"], sub["albedo"],
+            sub["specular_albedo"], sub["roughness"], d["envmap"], d["light2obj_rotmat"], faces, tri, bary, bits,
+            False)
+        genv.append(gk[5][0].reshape(-1).cpu().numpy())
+    out["ref_genv"] = np.stack(genv)
+    # no-visibility kernels: 6 axis points
+    n6 = d["normal"][:6].contiguous()
+    a6 = torch.ones(6, 3, device="cuda")
+    z6 = torch.zeros(6, 3, device="cuda")
+    r6 = torch.full((6, 1), 0.5, device="cuda")
+    g6 = ref.bruteforce_specular_shader_backward2(z6, torch.ones(6, 3, device="cuda"), n6, n6, a6, z6, r6,
+                                                  d["envmap"], d["light2obj_rotmat"], False)
+    out["ref_genv_novis"] = g6[5][0].reshape(-1).cpu().numpy()
+    if one_hot_env:
+        wn = np.zeros((HW, 6), dtype=np.float32)
+        for t in range(HW):
+            env = torch.zeros(3, H, W, device="cuda")
+            env.view(3, -1)[:, t] = 1.0
+            _, w = ref.bruteforce_specular_shader_forward2(n6, n6, a6, z6, r6, env, d["light2obj_rotmat"], False)
+            wn[t] = w[:, 0].cpu().numpy()
+        out["ref_white_novis"] = wn
+    torch.cuda.synchronize()
+    return out
 
 
 if __name__ == "__main__":
