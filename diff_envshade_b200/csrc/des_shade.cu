@@ -27,7 +27,10 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
 #include <mutex>
+#include <tuple>
+#include <utility>
 
 #include "des_math.cuh"
 #include "des_internal.h"
@@ -658,12 +661,37 @@ DeviceInfo device_info(int dev) {
   return cache[dev];
 }
 
+// Resident CTAs per SM of `kernel` at this block size and dynamic shared memory, cached per
+// (device, kernel, threads, smem); also opts the kernel in to that much dynamic shared memory on
+// the current device (once per raise).  Host-side only; keeps per-call overhead to a map lookup.
 template <typename K>
 int occupancy(K kernel, int threads, size_t smem) {
-  // opt in to the dynamic shared memory this launch needs (idempotent)
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  struct Key {
+    int dev;
+    const void* fn;
+    int threads;
+    size_t smem;
+    bool operator<(const Key& o) const {
+      return std::tie(dev, fn, threads, smem) < std::tie(o.dev, o.fn, o.threads, o.smem);
+    }
+  };
+  static std::mutex mu;
+  static std::map<Key, int> occ_cache;
+  static std::map<std::pair<int, const void*>, size_t> optin;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const Key key{dev, reinterpret_cast<const void*>(kernel), threads, smem};
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = occ_cache.find(key);
+  if (it != occ_cache.end()) return it->second;
+  size_t& granted = optin[{dev, key.fn}];
+  if (smem > granted) {
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    granted = smem;
+  }
   int nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess) return 0;
+  occ_cache[key] = nb;
   return nb;
 }
 
