@@ -212,6 +212,7 @@ def main():
         pg = dist
     import diff_envshade_b200 as des
     from diff_envshade_b200 import workloads as wl
+    from diff_envshade_b200.sharding import allreduce_env_grad
 
     c = wl.CONFIGS[CONFIG_NAME]
     inp_host = wl.make_inputs(c["P"], c["H"], c["W"], c["seed"] + 1000 * rank, sigma=c["sigma"], rough=c["rough"],
@@ -227,8 +228,7 @@ def main():
         g = des.bruteforce_specularvisibility_shader_backward2(
             d.grad_shading, d.grad_diffuse_shading, d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness,
             d.envmap, d.light2obj_rotmat, *vis, True)
-        if pg is not None:
-            pg.all_reduce(g[5])
+        allreduce_env_grad(g[5])
         return sh, wh, g
 
     for _ in range(args.warmup):
@@ -259,8 +259,7 @@ def main():
             d.grad_shading, d.grad_diffuse_shading, d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness,
             d.envmap, d.light2obj_rotmat, *vis, True)
         des.set_timing_events(0, 0)
-        if pg is not None:
-            pg.all_reduce(g[5])
+        allreduce_env_grad(g[5])
         ev[i][1].record()
     torch.cuda.synchronize()
     if pg is not None:
@@ -297,8 +296,7 @@ def main():
                                visibility=(t["face_vertex_list"], t["nearest_triangle_id"], t["barycentric_coord"],
                                            t["visibility"]))
             torch.autograd.backward([sh, wh], [t["grad_shading"], t["grad_diffuse_shading"]])
-            if pg is not None:
-                pg.all_reduce(t["envmap"].grad)
+            allreduce_env_grad(t["envmap"].grad)
             outs = [sh.detach(), wh.detach()] + [t[k].grad for k in ("normal", "view_dir", "albedo",
                                                                      "specular_albedo", "roughness", "envmap")]
             if out_host is None:
