@@ -94,6 +94,22 @@ int des_shade_backward(const des_shade_args* args, unsigned flags, const float* 
                        float* g_specular_albedo, float* g_roughness, float* g_envmap, void* workspace,
                        size_t workspace_bytes, des_stream_t stream);
 
+/* Size of the static device scratch array used by des_shade_backward_noalloc. */
+#define DES_SHADE_NOALLOC_SCRATCH_BYTES (4u << 20)
+
+/* des_shade_backward for callers that cannot allocate device memory (no counterpart in the
+ * reference).  Same inputs and outputs as des_shade_backward, no workspace argument: scratch comes
+ * from a library-owned static device array of DES_SHADE_NOALLOC_SCRATCH_BYTES, held on every GPU
+ * that uses it until the process exits.  Returns DES_ERR_WORKSPACE, without launching anything,
+ * when des_shade_workspace_bytes(P, H, W, flags, 1, device) exceeds that size.  All calls share the
+ * array: calls whose work overlaps on the GPU race and corrupt each other.  The first call on each
+ * device looks up the array's address (cudaGetSymbolAddress); make it before any stream capture.
+ * Allocates nothing. */
+int des_shade_backward_noalloc(const des_shade_args* args, unsigned flags, const float* grad_shading,
+                               const float* grad_diffuse_shading, float* g_normal, float* g_view_dir,
+                               float* g_albedo, float* g_specular_albedo, float* g_roughness, float* g_envmap,
+                               des_stream_t stream);
+
 /* The rotated texel table the kernels integrate over, written to table_out[H*W x 4] as
  * (x, y, z, d_omega) per texel in memory order.  Bit-exact with the reference's per-pair
  * getLightDir / getDeltaOmega / rotation (bruteforce_shader.cu:124-147, 2174-2197). */
