@@ -37,6 +37,7 @@ from ._C import (  # noqa: E402,F401  reference operator surface
     texel_table,
     workspace_bytes,
     set_timing_events,
+    relight_multienv,
 )
 from .autograd import (  # noqa: E402,F401
     DiffuseShade,
@@ -65,6 +66,7 @@ __all__ = [
     "bruteforce_specularvisibility_shader_backward2",
     "texel_table",
     "workspace_bytes",
+    "relight_multienv",
     "DiffuseShade",
     "SpecularShade",
     "SpecularShadeClamp",

@@ -126,6 +126,22 @@ int des_shade_backward(const des_shade_args* args, unsigned flags, const float* 
   return des::launch_shade(c, stream);
 }
 
+size_t des_relight_workspace_bytes(int64_t P, int32_t H, int32_t W, int32_t K) {
+  if ((int64_t)H * W > kMaxTexels) return 0;
+  return des::relight_workspace_bytes(P, H, W, K);
+}
+
+int des_relight_multienv(const des_shade_args* args, const float* envmaps, int32_t K, unsigned flags, float* out,
+                         void* workspace, size_t workspace_bytes, des_stream_t stream) {
+  if (args == nullptr || envmaps == nullptr || K <= 0) return DES_ERR_INVALID_ARGUMENT;
+  des_shade_args a = *args;
+  a.envmap = envmaps;  // validated like a single map; the relight path reads all K of them
+  int st = validate(&a, flags & ~(unsigned)DES_RELIGHT_BF16, false, out);
+  if (st != DES_OK) return st;
+  return des::launch_relight(a, envmaps, K, flags, out, workspace, workspace_bytes,
+                             reinterpret_cast<cudaStream_t>(stream));
+}
+
 int des_texel_table(int32_t H, int32_t W, const float* light2obj_rotmat, float* table_out, des_stream_t stream) {
   if (H <= 0 || W <= 0 || (int64_t)H * W > kMaxTexels || light2obj_rotmat == nullptr || table_out == nullptr)
     return DES_ERR_INVALID_ARGUMENT;
@@ -147,7 +163,7 @@ int des_workspace_status(void* workspace, size_t workspace_bytes, int* status_ou
     return DES_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return DES_ERR_CUDA;
   if (cudaMemsetAsync(ctrl + des::kCtrlError, 0, sizeof(unsigned), s) != cudaSuccess) return DES_ERR_CUDA;
-  *status_out = err ? DES_ERR_BAD_INDEX : DES_OK;
+  *status_out = (err & 2u) ? DES_ERR_TIMEOUT : (err ? DES_ERR_BAD_INDEX : DES_OK);
   return DES_OK;
 }
 

@@ -77,6 +77,12 @@ size_t workspace_bytes(const LaunchPlan& lp, bool backward, int grid);
 int shade_grid(const LaunchPlan& lp, unsigned flags, bool backward, bool vis);
 int launch_shade(const ShadeCall& call, des_stream_t stream);
 int launch_texel_table(int H, int W, const float* R, float* out, des_stream_t stream);
+// Texel records (see des_table_kernel) for an env map; also resets the workspace control words.
+int launch_table(int H, int W, int HWpad, const float* R, const float* env, float4* rec, unsigned* ctrl,
+                 cudaStream_t stream);
 void set_timing_events(cudaEvent_t start, cudaEvent_t stop);
+size_t relight_workspace_bytes(int64_t P, int H, int W, int K);
+int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigned flags, float* out, void* ws,
+                   size_t ws_bytes, cudaStream_t stream);
 
 }  // namespace des

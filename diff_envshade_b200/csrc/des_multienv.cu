@@ -1,0 +1,583 @@
+// Multi-env-map relighting on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// out[p, k, c] = sum_t A_c[p, t] * L_k[c, t],   A_c = albedo_c * w_d + specular_c * w_s,
+// where w_d = vis * max(n.l, 0) * dw / pi and w_s = vis * dw * F G D / 4 are the per-(point, texel)
+// weights of the reference's forward sum (bruteforce_shader.cu:2171-2236).  For one env map this is
+// the shading output of bruteforce_specularvisibility_shader_forward2; for K env maps it is, per
+// colour channel, a [points x texels] x [texels x K] product, which runs on the tensor cores.
+//
+// Precision: the weights are computed in FP32 and split into BF16 hi + lo parts, the radiance too;
+// each tile accumulates hi*hi + lo*hi + hi*lo in FP32 (error ~2^-16 relative).  DES_RELIGHT_BF16
+// keeps only hi*hi (plain BF16 inputs, error ~2^-8 relative per term).
+//
+// Kernel structure (one persistent CTA per SM, 14 warps):
+//   warps 0-7   builders: per 32-texel stage, 128 points x 32 texels of A_c (3 channels, hi and lo)
+//               written to shared memory in the UMMA K-major no-swizzle canonical layout
+//               (8-row x 16-byte core matrices, 128 B each);
+//   warp 8      allocates 512 TMEM columns; lane 0 issues tcgen05.mma (M=128, N=Kpad, K=16) and
+//               tcgen05.commit to the stage-empty / accumulator-full mbarriers;
+//   warps 9-12  epilogue: tcgen05.ld of the finished tile (32 TMEM lanes per warp) -> global;
+//   warp 13     lane 0 streams the prepared BF16 radiance tile of each stage with cp.async.bulk
+//               (a plain bulk copy from this GPU's memory; no multicast).
+// Two shared-memory stages and two TMEM accumulator buffers (2 x 3 x Kpad columns) let the weight
+// build, the MMAs and the epilogue overlap.  Every mbarrier wait is bounded (2 s of %globaltimer):
+// on timeout the CTA sets the workspace error word, stops issuing work, waits (bounded) for its
+// own bulk copies and MMAs in flight, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "des_internal.h"
+#include "des_math.cuh"
+#include "des_point.cuh"
+#include "diff_envshade_b200.h"
+
+namespace des {
+namespace relight {
+
+constexpr int kTileM = 128;                  // points per tile (UMMA M)
+constexpr int kStageT = 32;                  // texels per stage (one visibility slot)
+constexpr int kNStage = 2;                   // shared-memory ring depth
+constexpr int kEnvBlock = 64;                // env maps per pass
+constexpr int kBuilderThreads = 256;         // warps 0-7
+constexpr int kCtrlWarp = 8;
+constexpr int kEpiWarp0 = 9;                 // warps 9-12
+constexpr int kProdWarp = 13;
+constexpr int kThreads = 14 * 32;
+constexpr uint32_t kTmemCols = 512;
+constexpr int kATile = kTileM * kStageT * 2;  // bytes of one BF16 [128 x 32] operand tile
+constexpr long long kWaitNs = 2000000000LL;
+constexpr unsigned kErrTimeout = 2u;
+
+struct Params {
+  ShadeParams pt;         // point inputs, texel table, control words
+  const uint8_t* bprep;   // [nst][3][2][kpad x 32] BF16 radiance tiles (canonical layout)
+  float* out;             // [P][ldo]; this pass writes columns 3*kbase .. 3*(kbase + kblock) - 1
+  int64_t ldo;
+  int kbase, kblock, kpad, nst, ntiles;
+  bool split, vec_store;
+};
+
+struct Smem {  // byte offsets into dynamic shared memory
+  uint32_t tab, a, b, bar, misc, total;
+};
+
+__host__ __device__ inline uint32_t align_to(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+
+__host__ __device__ inline Smem smem_layout(int HWpad, int kpad) {
+  Smem s;
+  s.tab = 0;
+  s.a = align_to((uint32_t)HWpad * 32, 1024);
+  s.b = s.a + kNStage * 3 * 2 * kATile;
+  s.bar = align_to(s.b + kNStage * 3 * 2 * (uint32_t)kpad * kStageT * 2, 64);
+  s.misc = s.bar + 16 * 8;
+  s.total = s.misc + 64;
+  return s;
+}
+
+__host__ __device__ inline uint32_t bprep_stage_bytes(int kpad) { return 3u * 2u * (uint32_t)kpad * kStageT * 2u; }
+
+// ---- PTX helpers --------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity.  Returns false when this or another role of
+// the CTA gave up (shared abort flag); a timeout sets the workspace error word.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, unsigned* err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = global_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 0u) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > kWaitNs) {
+        *abort_flag = 1;
+        atomicOr(err, kErrTimeout);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// UMMA shared-memory descriptor, K-major, no swizzle: start, leading (K) and stride (M/N) byte offsets.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: BF16 x BF16 -> F32, both operands K-major, M x N.
+__host__ __device__ inline uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Byte offset of element (row r, texel j) in a K-major canonical [rows x 32] BF16 tile.
+__host__ __device__ inline uint32_t canon_off(int r, int j) {
+  return (uint32_t)(((r >> 3) * 4 + (j >> 3)) * 128 + (r & 7) * 16 + (j & 7) * 2);
+}
+
+// BF16 hi/lo split of two floats packed as bf16x2 (element 0 in the low half).
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+// ---- radiance preparation ------------------------------------------------------------------
+
+// bprep[st][c][hl][canon(k, j)] = hi/lo BF16 of L[kbase + k][c][st*32 + j] (zero outside the map / block).
+__global__ void prep_kernel(const float* __restrict__ env, int HW, int nst, int kbase, int kblock, int kpad,
+                            uint8_t* __restrict__ bprep) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // over nst * 3 * kpad * 32
+  const int total = nst * 3 * kpad * kStageT;
+  if (idx >= total) return;
+  const int j = idx % kStageT;
+  const int k = (idx / kStageT) % kpad;
+  const int c = (idx / (kStageT * kpad)) % 3;
+  const int st = idx / (kStageT * kpad * 3);
+  const int t = st * kStageT + j;
+  float L = 0.f;
+  if (k < kblock && t < HW) L = env[((size_t)(kbase + k) * 3 + c) * HW + t];
+  const __nv_bfloat16 hi = __float2bfloat16_rn(L);
+  const __nv_bfloat16 lo = __float2bfloat16_rn(L - __bfloat162float(hi));
+  const size_t tile = (size_t)kpad * kStageT * 2;
+  uint8_t* base = bprep + (size_t)st * bprep_stage_bytes(kpad) + (size_t)c * 2 * tile;
+  *reinterpret_cast<__nv_bfloat16*>(base + canon_off(k, j)) = hi;
+  *reinterpret_cast<__nv_bfloat16*>(base + tile + canon_off(k, j)) = lo;
+}
+
+// ---- main kernel ---------------------------------------------------------------------------
+
+template <bool DIFF, bool SPEC, bool VIS>
+__global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int HWpad = p.pt.HWpad;
+  const Smem L = smem_layout(HWpad, p.kpad);
+  float4* s_tab = reinterpret_cast<float4*>(smem + L.tab);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar);
+  uint64_t* full_a = bars;          // [2] builders -> MMA
+  uint64_t* full_b = bars + 2;      // [2] producer (tx bytes) -> MMA
+  uint64_t* empty = bars + 4;       // [2] MMA commit -> builders, producer
+  uint64_t* acc_full = bars + 6;    // [2] MMA commit -> epilogue
+  uint64_t* acc_empty = bars + 8;   // [2] epilogue -> MMA
+  uint64_t* drain = bars + 10;      // final MMA drain
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + L.misc);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.misc + 8);
+  unsigned* err = &p.pt.ctrl[kCtrlError];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t a_base = smem_u32(smem + L.a);
+  const uint32_t b_base = smem_u32(smem + L.b);
+  const uint32_t b_tile = (uint32_t)p.kpad * kStageT * 2;
+  const uint32_t b_stage = bprep_stage_bytes(p.kpad);
+
+  stage_table(s_tab, p.pt.table, 0, HWpad);
+  if (threadIdx.x == 0) {
+    mbar_init(&full_a[0], kBuilderThreads);
+    mbar_init(&full_a[1], kBuilderThreads);
+    mbar_init(&full_b[0], 1);
+    mbar_init(&full_b[1], 1);
+    mbar_init(&empty[0], 1);
+    mbar_init(&empty[1], 1);
+    mbar_init(&acc_full[0], 1);
+    mbar_init(&acc_full[1], 1);
+    mbar_init(&acc_empty[0], 128);
+    mbar_init(&acc_empty[1], 128);
+    mbar_init(drain, 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == kCtrlWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  if (threadIdx.x < kBuilderThreads) {
+    // ------------------------------------------------------------------ weight builders
+    const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
+    const bool need_view = SPEC || p.pt.clamp;
+    uint32_t q = 0;
+    for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
+      const int64_t pid = (int64_t)tile * kTileM + row;
+      const bool valid = pid < p.pt.P;
+      const PointGeom g = load_geom<VIS>(p.pt, pid, valid, need_view);
+      SpecConst sc;
+      if (SPEC) sc = spec_const(valid ? p.pt.rough[pid] : 0.f, g);
+      float alb[3] = {0.f, 0.f, 0.f}, spc[3] = {0.f, 0.f, 0.f};
+      if (valid) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (DIFF) alb[c] = p.pt.albedo[3 * pid + c];
+          if (SPEC) spc[c] = p.pt.spec[3 * pid + c];
+        }
+      }
+      for (int st = 0; st < p.nst; ++st, ++q) {
+        const uint32_t b = q & 1u, u = q >> 1;
+        uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
+        if (VIS) {
+          load_vis_words(p.pt, g, valid, st, w0, w1, w2);
+          w0 >>= 16 * half;
+          w1 >>= 16 * half;
+          w2 >>= 16 * half;
+        }
+        if (u > 0 && !mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err)) goto builders_done;
+        {
+          const uint32_t abuf = a_base + b * (3 * 2 * kATile);
+#pragma unroll
+          for (int j8 = 0; j8 < 2; ++j8) {
+            uint32_t hi[3][4], lo[3][4];
+#pragma unroll
+            for (int jj = 0; jj < 8; jj += 2) {
+              float av[3][2];
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int jl = j8 * 8 + jj + e;  // 0..15 within this thread's half stage
+                const int t = st * kStageT + half * 16 + jl;
+                const float4 A = s_tab[2 * t];
+                const float4 B = s_tab[2 * t + 1];
+                const float vis = VIS ? vis_weight(w0, w1, w2, 1u << jl, g.c0, g.c1, g.c2) : 1.f;
+                float wd, ws;
+                pair_fwd_weights<DIFF, SPEC>(g, sc, A, B.w, vis, wd, ws);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) av[c][e] = fmaf(alb[c], wd, spc[c] * ws);
+              }
+#pragma unroll
+              for (int c = 0; c < 3; ++c) split2(av[c][0], av[c][1], hi[c][jj / 2], lo[c][jj / 2]);
+            }
+            const int kc = half * 2 + j8;  // 8-texel chunk within the stage
+            const uint32_t off = (uint32_t)(((row >> 3) * 4 + kc) * 128 + (row & 7) * 16);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const uint32_t ahi = abuf + (uint32_t)(c * 2) * kATile + off;
+              asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ahi), "r"(hi[c][0]), "r"(hi[c][1]),
+                           "r"(hi[c][2]), "r"(hi[c][3])
+                           : "memory");
+              if (p.split)
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ahi + kATile), "r"(lo[c][0]),
+                             "r"(lo[c][1]), "r"(lo[c][2]), "r"(lo[c][3])
+                             : "memory");
+            }
+          }
+        }
+        fence_proxy_async_smem();
+        mbar_arrive(&full_a[b]);
+      }
+    }
+  builders_done:;
+  } else if (warp == kCtrlWarp) {
+    // ------------------------------------------------------------------ MMA issue (one thread)
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_bf16(kTileM, p.kpad);
+      uint32_t q = 0;
+      int i = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x, ++i) {
+        const uint32_t abuf = (uint32_t)i & 1u, au = (uint32_t)i >> 1;
+        if (au > 0 && !mbar_wait(&acc_empty[abuf], (au - 1) & 1u, s_abort, err)) break;
+        tc_fence_after();
+        for (int st = 0; st < p.nst; ++st, ++q) {
+          const uint32_t b = q & 1u, u = q >> 1;
+          if (!mbar_wait(&full_a[b], u & 1u, s_abort, err) || !mbar_wait(&full_b[b], u & 1u, s_abort, err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const uint32_t d = tmem + (abuf * 3u + (uint32_t)c) * (uint32_t)p.kpad;
+            const uint32_t ah = a_base + b * (3 * 2 * kATile) + (uint32_t)(c * 2) * kATile;
+            const uint32_t bh = b_base + b * b_stage + (uint32_t)(c * 2) * b_tile;
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+              const uint64_t da = umma_desc(ah + ks * 256, 128, 512);
+              const uint64_t db = umma_desc(bh + ks * 256, 128, 512);
+              umma_bf16(d, da, db, idesc, (st | ks) != 0 ? 1u : 0u);
+              if (p.split) {
+                umma_bf16(d, umma_desc(ah + kATile + ks * 256, 128, 512), db, idesc, 1u);
+                umma_bf16(d, da, umma_desc(bh + b_tile + ks * 256, 128, 512), idesc, 1u);
+              }
+            }
+          }
+          umma_commit(&empty[b]);
+        }
+        if (ok) umma_commit(&acc_full[abuf]);
+      }
+    }
+    __syncwarp();
+  } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
+    // ------------------------------------------------------------------ epilogue
+    const uint32_t quarter = (uint32_t)warp & 3u;  // TMEM lanes this warp may access
+    const int row = (int)quarter * 32 + lane;
+    int i = 0;
+    for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++i) {
+      const uint32_t abuf = (uint32_t)i & 1u, au = (uint32_t)i >> 1;
+      if (!mbar_wait(&acc_full[abuf], au & 1u, s_abort, err)) break;
+      tc_fence_after();
+      const int64_t pid = (int64_t)tile * kTileM + row;
+      float* orow = p.out + pid * p.ldo + (int64_t)p.kbase * 3;
+      for (int kb = 0; kb < p.kpad / 16; ++kb) {
+        float v[3][16];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          tmem_ld16(tmem + (quarter * 32u << 16) + (abuf * 3u + (uint32_t)c) * (uint32_t)p.kpad + kb * 16, v[c]);
+        tmem_wait_ld();
+        if (pid < p.pt.P) {
+          const int k0 = kb * 16;
+          if (p.vec_store && k0 + 16 <= p.kblock) {
+            float4* o4 = reinterpret_cast<float4*>(orow + k0 * 3);
+#pragma unroll
+            for (int i4 = 0; i4 < 12; ++i4) {
+              float x[4];
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const int f = i4 * 4 + e;
+                x[e] = v[f % 3][f / 3];
+              }
+              o4[i4] = make_float4(x[0], x[1], x[2], x[3]);
+            }
+          } else {
+#pragma unroll
+            for (int kk = 0; kk < 16; ++kk)
+              if (k0 + kk < p.kblock) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) orow[(k0 + kk) * 3 + c] = v[c][kk];
+              }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acc_empty[abuf]);
+    }
+  } else if (warp == kProdWarp) {
+    // ------------------------------------------------------------------ radiance bulk copies
+    if (lane == 0) {
+      uint32_t q = 0;
+      uint32_t last_use[2] = {0u, 0u};
+      bool issued[2] = {false, false};
+      for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
+        bool ok = true;
+        for (int st = 0; st < p.nst; ++st, ++q) {
+          const uint32_t b = q & 1u, u = q >> 1;
+          if (u > 0 && !mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&full_b[b], b_stage);
+          bulk_g2s(b_base + b * b_stage, p.bprep + (size_t)st * b_stage, b_stage, &full_b[b]);
+          issued[b] = true;
+          last_use[b] = u;
+        }
+        if (!ok) break;
+      }
+      // never leave a bulk copy in flight: wait (bounded) for the last one into each buffer
+      for (int b = 0; b < 2; ++b) {
+        if (!issued[b]) continue;
+        const long long t0 = global_ns();
+        while (!mbar_try_wait(&full_b[b], last_use[b] & 1u)) {
+          if (global_ns() - t0 > kWaitNs) {
+            atomicOr(err, kErrTimeout);
+            break;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  // ------------------------------------------------------------------ teardown
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kCtrlWarp) {
+    tc_fence_after();
+    if (lane == 0) {
+      // all MMAs this thread issued have completed before TMEM is freed
+      umma_commit(drain);
+      const long long t0 = global_ns();
+      while (!mbar_try_wait(drain, 0u)) {
+        if (global_ns() - t0 > kWaitNs) {
+          atomicOr(err, kErrTimeout);
+          break;
+        }
+      }
+    }
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
+}  // namespace relight
+
+// ---- host side -----------------------------------------------------------------------------
+
+namespace {
+
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+using RelightFn = void (*)(const relight::Params);
+
+RelightFn pick_relight(bool diff, bool spec, bool vis) {
+  using namespace relight;
+  if (diff) {
+    if (spec) return vis ? relight_kernel<true, true, true> : relight_kernel<true, true, false>;
+    return vis ? relight_kernel<true, false, true> : relight_kernel<true, false, false>;
+  }
+  return vis ? relight_kernel<false, true, true> : relight_kernel<false, true, false>;
+}
+
+int kpad_of(int kblock) { return std::max(16, (kblock + 15) / 16 * 16); }
+
+}  // namespace
+
+size_t relight_workspace_bytes(int64_t P, int H, int W, int K) {
+  if (P < 0 || H <= 0 || W <= 0 || K <= 0) return 0;
+  const int HWpad = (H * W + 31) / 32 * 32;
+  const int kpad = kpad_of(std::min(K, relight::kEnvBlock));
+  return kCtrlBytes + align256((size_t)HWpad * 32) + align256((size_t)(HWpad / 32) * relight::bprep_stage_bytes(kpad));
+}
+
+int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigned flags, float* out, void* ws,
+                   size_t ws_bytes, cudaStream_t stream) {
+  const bool diff = flags & DES_DIFFUSE, spec = flags & DES_SPECULAR;
+  const bool vis = a.visibility != nullptr;
+  const int HW = a.H * a.W;
+  const int HWpad = (HW + 31) / 32 * 32;
+  if (HWpad > 2048) return DES_ERR_UNSUPPORTED;  // the texel table must fit in shared memory
+  if (ws == nullptr || ws_bytes < relight_workspace_bytes(a.P, a.H, a.W, K) ||
+      (reinterpret_cast<uintptr_t>(ws) & 255u) != 0)
+    return DES_ERR_WORKSPACE;
+  int dev = 0, sms = 0, max_smem = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DES_ERR_CUDA;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+
+  uint8_t* w = static_cast<uint8_t*>(ws);
+  unsigned* ctrl = reinterpret_cast<unsigned*>(w);
+  float4* table = reinterpret_cast<float4*>(w + kCtrlBytes);
+  uint8_t* bprep = w + kCtrlBytes + align256((size_t)HWpad * 32);
+
+  int st = launch_table(a.H, a.W, HWpad, a.light2obj_rotmat, envmaps, table, ctrl, stream);
+  if (st != DES_OK) return st;
+  if (a.P == 0) return DES_OK;
+  if (!diff && !spec) {
+    return cudaMemsetAsync(out, 0, sizeof(float) * 3 * (size_t)K * a.P, stream) == cudaSuccess ? DES_OK : DES_ERR_CUDA;
+  }
+
+  relight::Params prm{};
+  ShadeParams& pt = prm.pt;
+  pt.P = a.P;
+  pt.HWpad = HWpad;
+  pt.chunk = HWpad;
+  pt.N_face = a.N_face;
+  pt.N_vertex = a.N_vertex;
+  pt.normal = a.normal;
+  pt.view = a.view_dir;
+  pt.albedo = a.albedo;
+  pt.spec = a.specular_albedo;
+  pt.rough = a.roughness;
+  pt.faces = a.face_vertex_list;
+  pt.tri = a.nearest_triangle_id;
+  pt.bary = a.barycentric_coord;
+  pt.vis = a.visibility;
+  pt.table = table;
+  pt.clamp = (flags & DES_CLAMP) != 0;
+  pt.ctrl = ctrl;
+  prm.bprep = bprep;
+  prm.out = out;
+  prm.ldo = 3 * (int64_t)K;
+  prm.nst = HWpad / relight::kStageT;
+  prm.ntiles = (int)((a.P + relight::kTileM - 1) / relight::kTileM);
+  prm.split = !(flags & DES_RELIGHT_BF16);
+
+  RelightFn k = pick_relight(diff, spec, vis);
+  const int grid = std::max(1, std::min(prm.ntiles, sms));
+  for (int kbase = 0; kbase < K; kbase += relight::kEnvBlock) {
+    prm.kbase = kbase;
+    prm.kblock = std::min(relight::kEnvBlock, K - kbase);
+    prm.kpad = kpad_of(prm.kblock);
+    prm.vec_store = ((reinterpret_cast<uintptr_t>(out) & 15u) == 0) && (prm.ldo % 4 == 0) && ((kbase * 3) % 4 == 0);
+    const relight::Smem L = relight::smem_layout(HWpad, prm.kpad);
+    if ((int)L.total > max_smem) return DES_ERR_UNSUPPORTED;
+    const int total = prm.nst * 3 * prm.kpad * relight::kStageT;
+    relight::prep_kernel<<<(total + 255) / 256, 256, 0, stream>>>(envmaps, HW, prm.nst, kbase, prm.kblock, prm.kpad,
+                                                                  bprep);
+    if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total) != cudaSuccess)
+      return DES_ERR_CUDA;
+    k<<<grid, relight::kThreads, L.total, stream>>>(prm);
+    if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+  }
+  return DES_OK;
+}
+
+}  // namespace des

@@ -364,6 +364,58 @@ std::vector<Tensor> bruteforce_specularvisibility_shader_backward2(
 // Extras (not in the reference)
 // ---------------------------------------------------------------------------------------------
 
+// Forward shading of P points under K env maps at once on the tensor cores: returns [P, K, 3].
+// envmaps: [K, 3, H, W].  Visibility inputs are optional (all four or none).  split=false uses
+// plain BF16 operands instead of the BF16 hi+lo split.
+Tensor relight_multienv(const Tensor& normal, const Tensor& view, const Tensor& albedo, const Tensor& spec,
+                        const Tensor& rough, const Tensor& envmaps, const Tensor& R,
+                        const c10::optional<Tensor>& faces, const c10::optional<Tensor>& tri,
+                        const c10::optional<Tensor>& bary, const c10::optional<Tensor>& vis, bool enable_specular,
+                        bool split) {
+  check_f32(envmaps, "envmaps");
+  TORCH_CHECK(envmaps.dim() == 4, "envmaps must have shape [K, C, H, W], got ", envmaps.sizes());
+  Common c = common_checks(normal, albedo, envmaps[0], R);
+  spec_checks(c, view, spec, rough);
+  const int64_t K = envmaps.size(0);
+  TORCH_CHECK(K > 0, "envmaps is empty");
+  const bool has_vis = vis.has_value();
+  TORCH_CHECK(faces.has_value() == has_vis && tri.has_value() == has_vis && bary.has_value() == has_vis,
+              "visibility inputs must be given together");
+  VisArgs v{0, 0, 0};
+  if (has_vis) v = vis_checks(c, *faces, *tri, *bary, *vis);
+  const at::cuda::OptionalCUDAGuard guard(device_of(normal));
+  Tensor out = torch::empty({c.P, K, c.C}, normal.options().requires_grad(false));
+  const size_t bytes = des_relight_workspace_bytes(c.P, c.H, c.W, (int)K);
+  TORCH_CHECK(bytes > 0, "diff_envshade_b200: could not size the relight workspace");
+  Tensor ws = torch::empty({(int64_t)bytes}, normal.options().dtype(torch::kUInt8));
+  des_shade_args a{};
+  a.P = c.P;
+  a.H = c.H;
+  a.W = c.W;
+  a.C = (int)c.C;
+  a.normal = fptr(normal);
+  a.view_dir = fptr(view);
+  a.albedo = fptr(albedo);
+  a.specular_albedo = fptr(spec);
+  a.roughness = fptr(rough);
+  a.light2obj_rotmat = fptr(R);
+  if (has_vis) {
+    a.N_face = v.N_face;
+    a.N_vertex = v.N_vertex;
+    a.N_slot = v.N_slot;
+    a.face_vertex_list = faces->data_ptr<int32_t>();
+    a.nearest_triangle_id = tri->data_ptr<int64_t>();
+    a.barycentric_coord = fptr(*bary);
+    a.visibility = reinterpret_cast<const uint32_t*>(vis->data_ptr<int32_t>());
+  }
+  unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u) | (split ? 0u : DES_RELIGHT_BF16);
+  auto stream = at::cuda::getCurrentCUDAStream().stream();
+  int st = des_relight_multienv(&a, fptr(envmaps), (int)K, f, fptr_mut(out), ws.data_ptr(), (size_t)ws.numel(),
+                                cur_stream());
+  finish(st, ws, stream);
+  return out;
+}
+
 // The rotated texel table the kernels integrate over: [H*W, 4] = (x, y, z, d_omega).
 Tensor texel_table(int64_t H, int64_t W, const Tensor& R) {
   check_f32(R, "light2obj_rotmat");
@@ -399,6 +451,11 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("bruteforce_specularvisibility_shader_forward2", &bruteforce_specularvisibility_shader_forward2, "bruteforce specular visibility shader forward2 (CUDA)");
   m.def("bruteforce_specularvisibility_shader_backward2", &bruteforce_specularvisibility_shader_backward2, "bruteforce specular visibility shader backward2 (CUDA)");
   m.def("texel_table", &texel_table, "rotated texel table [H*W, 4] = (x, y, z, d_omega)");
+  m.def("relight_multienv", &relight_multienv, "forward shading under K env maps on tcgen05 -> [P, K, 3]",
+        py::arg("normal"), py::arg("view_dir"), py::arg("albedo"), py::arg("specular_albedo"), py::arg("roughness"),
+        py::arg("envmaps"), py::arg("light2obj_rotmat"), py::arg("face_vertex_list") = py::none(),
+        py::arg("nearest_triangle_id") = py::none(), py::arg("barycentric_coord") = py::none(),
+        py::arg("visibility") = py::none(), py::arg("enable_specular") = true, py::arg("split") = true);
   m.def("workspace_bytes", &workspace_bytes, "scratch bytes of one shading call");
   m.def("set_timing_events", &set_timing_events, "bracket the main kernel of later calls with these CUDA events");
   m.attr("DES_DIFFUSE") = (int)DES_DIFFUSE;

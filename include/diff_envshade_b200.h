@@ -43,6 +43,7 @@ typedef enum des_status {
 #define DES_DIFFUSE 1u  /* Lambert term                                                 */
 #define DES_SPECULAR 2u /* GGX term (Schlick Fresnel, Schlick-Smith G, GGX NDF)          */
 #define DES_CLAMP 4u    /* backface clamp: a point with n.v <= 0 shades to zero          */
+#define DES_RELIGHT_BF16 8u /* des_relight_multienv: plain BF16 operands (default: BF16 hi+lo split) */
 
 /* All inputs of one shading call.  The visibility block is ignored when visibility == NULL. */
 typedef struct des_shade_args {
@@ -109,6 +110,22 @@ int des_shade_backward_noalloc(const des_shade_args* args, unsigned flags, const
                                const float* grad_diffuse_shading, float* g_normal, float* g_view_dir,
                                float* g_albedo, float* g_specular_albedo, float* g_roughness, float* g_envmap,
                                des_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Multi-env-map relighting (tensor cores)
+ * ------------------------------------------------------------------------------------- */
+
+/* Scratch bytes of des_relight_multienv for P points, an H x W map and K env maps. */
+size_t des_relight_workspace_bytes(int64_t P, int32_t H, int32_t W, int32_t K);
+
+/* out[P x K x 3] = the forward shading of the P points under each of K env maps
+ * (envmaps: K x 3 x H x W float32; args->envmap is ignored), i.e. K calls of the reference's
+ * bruteforce_specularvisibility_shader_forward2 (bruteforce_shader.cu:3261) -- or of
+ * bruteforce_specular_shader_forward2 without visibility -- fused into one pass whose
+ * point x texel weights are contracted with the K maps on tcgen05 (BF16 in, FP32 accumulate).
+ * flags: DES_DIFFUSE | DES_SPECULAR [| DES_CLAMP] [| DES_RELIGHT_BF16].  H*W <= 2048. */
+int des_relight_multienv(const des_shade_args* args, const float* envmaps, int32_t K, unsigned flags, float* out,
+                         void* workspace, size_t workspace_bytes, des_stream_t stream);
 
 /* The rotated texel table the kernels integrate over, written to table_out[H*W x 4] as
  * (x, y, z, d_omega) per texel in memory order.  Bit-exact with the reference's per-pair
