@@ -24,8 +24,10 @@ struct PointGeom {
 
 // Loads a lane's normal / view / visibility vertices.  Out-of-range triangle or vertex ids set
 // the workspace error bit and make the point inactive (it then shades to zero).
-template <bool VIS>
-__device__ __forceinline__ PointGeom load_geom(const ShadeParams& p, int64_t pid, bool valid, bool need_view) {
+// PP is any parameter struct with the members P, normal, view, tri, faces, N_face, N_vertex, bary,
+// clamp and ctrl (ShadeParams, or the serving request descriptor).
+template <bool VIS, class PP>
+__device__ __forceinline__ PointGeom load_geom(const PP& p, int64_t pid, bool valid, bool need_view) {
   PointGeom g;
   g.nx = g.ny = g.nz = 0.f;
   g.vx = g.vy = g.vz = 0.f;
@@ -64,7 +66,8 @@ __device__ __forceinline__ PointGeom load_geom(const ShadeParams& p, int64_t pid
   return g;
 }
 
-__device__ __forceinline__ void load_vis_words(const ShadeParams& p, const PointGeom& g, bool valid, int slot,
+template <class PP>
+__device__ __forceinline__ void load_vis_words(const PP& p, const PointGeom& g, bool valid, int slot,
                                                uint32_t& w0, uint32_t& w1, uint32_t& w2) {
   if (valid) {
     const uint32_t* row = p.vis + (int64_t)slot * p.N_vertex;
@@ -138,6 +141,187 @@ __device__ __forceinline__ void pair_fwd_weights(const PointGeom& g, const SpecC
     const float tmp = F * G * D * 0.25f;
     ws = (act && tmp > 0.f) ? tmp * A.w * vis : 0.f;
   }
+}
+
+
+// Incoming gradients of one point folded with its albedos (bruteforce_shader.cu:2585-2588):
+// gd = g_shading * albedo + g_diffuse_shading, gs = g_shading * specular_albedo.
+struct BwdPoint {
+  float gd0, gd1, gd2, gs0, gs1, gs2;
+};
+
+// Per-point sums of the fused adjoint (one set per lane; layout is relied on as 15 floats):
+// Da = sum L w_d (-> g_albedo), Sa = sum L w_s (-> g_specular_albedo), gn/gv = normal/view gradients
+// without the Schlick-Smith view factor, ga1 = d/dk, ga2 = d/d alpha^2, gbs = sum of d/db.
+struct BwdAcc {
+  float Da0, Da1, Da2, Sa0, Sa1, Sa2, gnx, gny, gnz, gvx, gvy, gvz, ga1, ga2, gbs;
+};
+
+// Adjoint of one (point, texel) pair: accumulates into `acc` and returns the pair's forward
+// weights (for the env-map gradient e_c = gd_c wd + gs_c ws).  bruteforce_shader.cu:2380-2484.
+template <bool DIFF, bool SPEC>
+__device__ __forceinline__ void pair_bwd(const PointGeom& g, const SpecConst& sc, const BwdPoint& gp, const float4& A,
+                                         const float4& B, float vis, BwdAcc& acc, float& wd_out, float& ws_out) {
+  const float nl = dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z);
+  const bool act = nl > 0.f;
+  wd_out = 0.f;
+  ws_out = 0.f;
+  if (DIFF) {
+    // Lambert adjoint (bruteforce_shader.cu:2413-2426)
+    const float wdv = act ? B.w * vis : 0.f;  // d_omega/pi * vis
+    const float wd = nl * wdv;
+    acc.Da0 = fmaf(B.x, wd, acc.Da0);
+    acc.Da1 = fmaf(B.y, wd, acc.Da1);
+    acc.Da2 = fmaf(B.z, wd, acc.Da2);
+    const float gdot = dot3(gp.gd0, gp.gd1, gp.gd2, B.x, B.y, B.z) * wdv;
+    acc.gnx = fmaf(gdot, A.x, acc.gnx);
+    acc.gny = fmaf(gdot, A.y, acc.gny);
+    acc.gnz = fmaf(gdot, A.z, acc.gnz);
+    wd_out = wd;
+  }
+  if (SPEC) {
+    const float hx = A.x + g.vx, hy = A.y + g.vy, hz = A.z + g.vz;
+    const float hh = fmaxf(dot3(hx, hy, hz, hx, hy, hz), kHalfVecFloor);
+    const float ri = rsqrt_approx(hh);
+    const float nh = dot3(g.nx, g.ny, g.nz, hx, hy, hz) * ri;
+    const float lh = dot3(A.x, A.y, A.z, hx, hy, hz) * ri;
+    const float a = 1.f - __saturatef(lh);
+    const float a2 = a * a;
+    const float a4 = a2 * a2;
+    const float F = fmaf(a4 * a, 1.f - kR0, kR0);
+    const float ia = rcp_approx(fmaf(nl, sc.omk, sc.k));
+    const float Ga = nl * ia;
+    const float G = Ga * sc.invB;
+    const float nh2 = nh * nh;
+    const float tt = ggx_t(g, hx, hy, hz, ri, nh2, sc);
+    const float t2 = kPiF * tt * tt;
+    const float itm = rcp_approx(fmaxf(t2, kThres));
+    const float D = sc.alpha2 * itm;
+    const float tmp = F * G * D * 0.25f;
+    const float wsv = (act && tmp > 0.f) ? A.w * vis : 0.f;  // d_omega * vis
+    const float ws = tmp * wsv;
+    acc.Sa0 = fmaf(B.x, ws, acc.Sa0);
+    acc.Sa1 = fmaf(B.y, ws, acc.Sa1);
+    acc.Sa2 = fmaf(B.z, ws, acc.Sa2);
+    ws_out = ws;
+    // d shading / d tmp, then split into F, G, D (bruteforce_shader.cu:2436-2445)
+    const float q = dot3(gp.gs0, gp.gs1, gp.gs2, B.x, B.y, B.z) * wsv * 0.25f;
+    const float gF = q * (G * D);
+    const float gG = q * (F * D);
+    const float gD = q * (F * G);
+    // Fresnel adjoint (bruteforce_shader.cu:155-159)
+    const float gch = (lh >= 0.f && lh <= 1.f) ? (5.f * (kR0 - 1.f)) * gF * a4 : 0.f;
+    float ghx = gch * A.x, ghy = gch * A.y, ghz = gch * A.z;
+    // Schlick-Smith adjoint, light side (bruteforce_shader.cu:173-201); the view side is
+    // linear in a per-point factor and is applied once per point after the loop
+    const float gA = gG * sc.invB;
+    const float ia2 = ia * ia;
+    const float gdln = gA * sc.k * ia2;
+    acc.gnx = fmaf(gdln, A.x, acc.gnx);
+    acc.gny = fmaf(gdln, A.y, acc.gny);
+    acc.gnz = fmaf(gdln, A.z, acc.gnz);
+    acc.ga1 = fmaf(gA * ia2, fmaf(nl, nl, -nl), acc.ga1);
+    acc.gbs = fmaf(-gA * Ga, sc.invB, acc.gbs);
+    // GGX NDF adjoint (bruteforce_shader.cu:212-227); 1/t = pi t / (pi t^2)
+    acc.ga2 = fmaf(gD, itm, acc.ga2);
+    const float gt = (t2 > kThres) ? (-2.f * kPiF) * sc.alpha2 * gD * tt * itm * itm : 0.f;
+    acc.ga2 = fmaf(nh2, gt, acc.ga2);
+    const float gdnh = 2.f * gt * sc.am1 * nh;
+    const float hnx = hx * ri, hny = hy * ri, hnz = hz * ri;
+    acc.gnx = fmaf(gdnh, hnx, acc.gnx);
+    acc.gny = fmaf(gdnh, hny, acc.gny);
+    acc.gnz = fmaf(gdnh, hnz, acc.gnz);
+    ghx = fmaf(gdnh, g.nx, ghx);
+    ghy = fmaf(gdnh, g.ny, ghy);
+    ghz = fmaf(gdnh, g.nz, ghz);
+    // normalize adjoint (bruteforce_shader.cu:63-71) and h = l + v -> v
+    const float hg = dot3(hnx, hny, hnz, ghx, ghy, ghz);
+    acc.gvx = fmaf(fmaf(-hnx, hg, ghx), ri, acc.gvx);
+    acc.gvy = fmaf(fmaf(-hny, hg, ghy), ri, acc.gvy);
+    acc.gvz = fmaf(fmaf(-hnz, hg, ghz), ri, acc.gvz);
+  }
+}
+
+// Transposing butterfly: e[j] (j = 0..7) per lane -> every lane holds the 32-lane sum of texel
+// 4*b4 + 2*b3 + b2 of its lane id (b4 = bit 4, ...), identical in lanes that differ in bits 0-1.
+__device__ __forceinline__ float butterfly8(const float (&e)[8], int lane) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  float x[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float keep = b4 ? e[i + 4] : e[i];
+    const float send = b4 ? e[i] : e[i + 4];
+    x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  float y[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const float keep = b3 ? x[i + 2] : x[i];
+    const float send = b3 ? x[i] : x[i + 2];
+    y[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  float z;
+  {
+    const float keep = b2 ? y[1] : y[0];
+    const float send = b2 ? y[0] : y[1];
+    z = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  return z;
+}
+
+
+// Outputs of the fused adjoint (any of the last four may be null).
+struct BwdOutputs {
+  float *g_normal, *g_view, *g_albedo, *g_spec, *g_rough;
+};
+
+// Finishes one point from its reduced adjoint sums (BwdAcc order): applies the Schlick-Smith view
+// factor (bruteforce_shader.cu:194-200) and the roughness chain rule (2501-2502) and stores the
+// point's gradients.  r = roughness, g_shading3 = the point's incoming shading gradient.
+template <bool DIFF, bool SPEC>
+__device__ __forceinline__ void finish_bwd_point(const float (&sums)[15], const PointGeom& g, const SpecConst& sc,
+                                                 float r, const float* g_shading3, int64_t pid, const BwdOutputs& o) {
+  float n_x = sums[6], n_y = sums[7], n_z = sums[8];
+  float v_x = sums[9], v_y = sums[10], v_z = sums[11];
+  float g_rough = 0.f;
+  if (SPEC) {
+    // view side of the Schlick-Smith adjoint (bruteforce_shader.cu:194-200)
+    const float gdvn = sums[14] * sc.omk;
+    if (sc.nvp > 0.f) {
+      v_x = fmaf(gdvn, g.nx, v_x);
+      v_y = fmaf(gdvn, g.ny, v_y);
+      v_z = fmaf(gdvn, g.nz, v_z);
+      n_x = fmaf(gdvn, g.vx, n_x);
+      n_y = fmaf(gdvn, g.vy, n_y);
+      n_z = fmaf(gdvn, g.vz, n_z);
+    }
+    const float gk = fmaf(sums[14], 1.f - sc.nvp, sums[12]);
+    // roughness chain rule (bruteforce_shader.cu:2501-2502)
+    g_rough = sums[13] * 4.f * r * r * r;
+    g_rough += gk * (1.f + r) / 4.f;
+  }
+  o.g_normal[3 * pid] = n_x;
+  o.g_normal[3 * pid + 1] = n_y;
+  o.g_normal[3 * pid + 2] = n_z;
+  const float g0 = g_shading3[0], g1 = g_shading3[1], g2 = g_shading3[2];
+  if (o.g_albedo != nullptr) {
+    o.g_albedo[3 * pid] = DIFF ? g0 * sums[0] : 0.f;
+    o.g_albedo[3 * pid + 1] = DIFF ? g1 * sums[1] : 0.f;
+    o.g_albedo[3 * pid + 2] = DIFF ? g2 * sums[2] : 0.f;
+  }
+  if (o.g_spec != nullptr) {
+    o.g_spec[3 * pid] = SPEC ? g0 * sums[3] : 0.f;
+    o.g_spec[3 * pid + 1] = SPEC ? g1 * sums[4] : 0.f;
+    o.g_spec[3 * pid + 2] = SPEC ? g2 * sums[5] : 0.f;
+  }
+  if (o.g_view != nullptr) {
+    o.g_view[3 * pid] = SPEC ? v_x : 0.f;
+    o.g_view[3 * pid + 1] = SPEC ? v_y : 0.f;
+    o.g_view[3 * pid + 2] = SPEC ? v_z : 0.f;
+  }
+  if (o.g_rough != nullptr) o.g_rough[pid] = g_rough;
 }
 
 }  // namespace des

@@ -1,0 +1,956 @@
+// Serving: continuous batching of shading requests onto the GPU.
+//
+// Requests (forward, or forward + adjoint) of any point count arrive asynchronously.  A native
+// scheduler thread
+//   * admits them in arrival order while a device arena of fixed size (the HBM budget) has room,
+//     skipping over requests that do not fit yet, and uploads their point data on a copy stream;
+//   * keeps env maps (their texel tables) and meshes (faces + visibility words) resident, shared by
+//     reference between requests;
+//   * every tick packs 32-point tiles of the admitted requests into a work list, smallest
+//     remaining work first, up to a time budget, and launches it as a CUDA graph (work-list upload
+//     + one persistent batch kernel) on one of two compute streams, so consecutive ticks overlap;
+//   * when every tile of a request has finished, copies its outputs back and frees its memory.
+// Work of different requests therefore shares each launch and each SM; a request that arrives
+// while others run joins the next tick.
+//
+// The batch kernel evaluates exactly the per-pair arithmetic of des_fwd_kernel / des_bwd_kernel
+// (shared helpers in des_point.cuh); per-point outputs are bit-identical to a solo call of the
+// batch path, and the env-map gradient is summed per request in FP64 (global FP64 atomics, then a
+// final FP32 conversion by whichever CTA finishes the request's last adjoint tile).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "des_internal.h"
+#include "des_math.cuh"
+#include "des_point.cuh"
+#include "diff_envshade_b200.h"
+
+namespace des {
+namespace serve {
+
+constexpr int kNW = 8;               // warps per CTA
+constexpr int kMaxHWpad = 2048;      // texel table kept in shared memory per CTA
+constexpr int kMaxSlots = 8192;      // concurrently admitted requests
+constexpr int kTickItems = 4096;     // work items per tick (upper bound; the whole list is uploaded)
+constexpr int kNTicks = 4;           // tick buffers (up to this many ticks in flight)
+
+// Device-side request descriptor (member names shared with ShadeParams for the point loaders).
+struct ReqDesc {
+  int64_t P;
+  int HW, HWpad;
+  int diff, spec, has_vis;
+  bool clamp;
+  const float* normal;
+  const float* view;
+  const float* albedo;
+  const float* spec_alb;
+  const float* rough;
+  const float4* table;
+  int N_face, N_vertex;
+  const int32_t* faces;
+  const int64_t* tri;
+  const float* bary;
+  const uint32_t* vis;
+  const float* g_shading;
+  const float* g_white;
+  float* shading;
+  float* white;
+  float* g_normal;
+  float* g_view;
+  float* g_albedo;
+  float* g_spec;
+  float* g_rough;
+  float* g_env;
+  double* env_acc;           // [3][HWpad], zeroed at admission
+  unsigned* bwd_tiles_left;  // adjoint tiles not yet finished
+  unsigned* ctrl;            // [kCtrlError] = error word
+};
+
+struct WorkItem {
+  int32_t req, tile, kind, pad;  // kind 0 = forward tile, 1 = adjoint tile
+};
+
+// Pinned host staging of one slot's uploads (stays valid while the slot's request is admitted).
+struct SlotStage {
+  ReqDesc desc;
+  unsigned tiles_left;
+  unsigned pad[3];
+};
+
+struct WorkList {
+  unsigned counter, n, pad0, pad1;
+  WorkItem items[kTickItems];
+};
+
+// ---------------------------------------------------------------------------------------------
+// Batch kernel
+// ---------------------------------------------------------------------------------------------
+
+template <bool DIFF, bool SPEC, bool VIS>
+__device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t pid = (int64_t)tile * 32 + lane;
+  const bool valid = pid < r.P;
+  const PointGeom g = load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
+  SpecConst sc;
+  if (SPEC) sc = spec_const(valid ? r.rough[pid] : 0.f, g);
+  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  const int nsl = r.HWpad >> 5;
+  const int sl0 = (warp * nsl) / kNW, sl1 = ((warp + 1) * nsl) / kNW;
+  for (int sl = sl0; sl < sl1; ++sl) {
+    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
+    if (VIS) {
+      load_vis_words(r, g, valid, sl, w0, w1, w2);
+      if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
+    }
+    const float4* rec = s_tab + 2 * (sl << 5);
+#pragma unroll 1
+    for (int gq = 0; gq < 4; ++gq) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float4 A = rec[2 * (gq * 8 + j)];
+        const float4 B = rec[2 * (gq * 8 + j) + 1];
+        const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
+        float wd, ws;
+        pair_fwd_weights<DIFF, SPEC>(g, sc, A, B.w, vis, wd, ws);
+        acc[0] = fmaf(B.x, wd, acc[0]);
+        acc[1] = fmaf(B.y, wd, acc[1]);
+        acc[2] = fmaf(B.z, wd, acc[2]);
+        acc[3] = fmaf(B.x, ws, acc[3]);
+        acc[4] = fmaf(B.y, ws, acc[4]);
+        acc[5] = fmaf(B.z, ws, acc[5]);
+      }
+      if (VIS) {
+        w0 >>= 8;
+        w1 >>= 8;
+        w2 >>= 8;
+      }
+    }
+  }
+  float* red = s_red + warp * 6 * 32 + lane;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) red[q * 32] = acc[q];
+  __syncthreads();
+  if (warp == 0 && valid) {
+    float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int w = 0; w < kNW; ++w)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) s[q] += s_red[w * 6 * 32 + q * 32 + lane];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float out = 0.f;
+      if (DIFF) out = r.albedo[3 * pid + c] * s[c];
+      if (SPEC) out = fmaf(r.spec_alb[3 * pid + c], s[3 + c], out);
+      r.shading[3 * pid + c] = out;
+      if (r.white != nullptr) r.white[3 * pid + c] = s[c];
+    }
+  }
+}
+
+template <bool DIFF, bool SPEC, bool VIS>
+__device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
+  constexpr int NACC = 15;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t pid = (int64_t)tile * 32 + lane;
+  const bool valid = pid < r.P;
+  const PointGeom g = load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
+  float gd0 = 0.f, gd1 = 0.f, gd2 = 0.f, gs0 = 0.f, gs1 = 0.f, gs2 = 0.f;
+  if (valid) {
+    const float g0 = r.g_shading[3 * pid], g1 = r.g_shading[3 * pid + 1], g2 = r.g_shading[3 * pid + 2];
+    if (DIFF) {
+      gd0 = g0 * r.albedo[3 * pid];
+      gd1 = g1 * r.albedo[3 * pid + 1];
+      gd2 = g2 * r.albedo[3 * pid + 2];
+      if (r.g_white != nullptr) {
+        gd0 += r.g_white[3 * pid];
+        gd1 += r.g_white[3 * pid + 1];
+        gd2 += r.g_white[3 * pid + 2];
+      }
+    }
+    if (SPEC) {
+      gs0 = g0 * r.spec_alb[3 * pid];
+      gs1 = g1 * r.spec_alb[3 * pid + 1];
+      gs2 = g2 * r.spec_alb[3 * pid + 2];
+    }
+  }
+  SpecConst sc;
+  if (SPEC) sc = spec_const(valid ? r.rough[pid] : 0.f, g);
+  const BwdPoint gp{gd0, gd1, gd2, gs0, gs1, gs2};
+  BwdAcc acc = {};
+  const int nsl = r.HWpad >> 5;
+  const int sl0 = (warp * nsl) / kNW, sl1 = ((warp + 1) * nsl) / kNW;
+  const int jsel = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+  for (int sl = sl0; sl < sl1; ++sl) {
+    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
+    if (VIS) {
+      load_vis_words(r, g, valid, sl, w0, w1, w2);
+      if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
+    }
+    const float4* rec = s_tab + 2 * (sl << 5);
+#pragma unroll 1
+    for (int gq = 0; gq < 4; ++gq) {
+      float wdj[8], wsj[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float4 A = rec[2 * (gq * 8 + j)];
+        const float4 B = rec[2 * (gq * 8 + j) + 1];
+        const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
+        pair_bwd<DIFF, SPEC>(g, sc, gp, A, B, vis, acc, wdj[j], wsj[j]);
+      }
+      if (VIS) {
+        w0 >>= 8;
+        w1 >>= 8;
+        w2 >>= 8;
+      }
+      float e[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) e[j] = fmaf(gs0, wsj[j], gd0 * wdj[j]);
+      const float y0 = butterfly8(e, lane);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) e[j] = fmaf(gs1, wsj[j], gd1 * wdj[j]);
+      const float y1 = butterfly8(e, lane);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) e[j] = fmaf(gs2, wsj[j], gd2 * wdj[j]);
+      const float y2 = butterfly8(e, lane);
+      if ((lane & 3) == 0) {
+        const int t = (sl << 5) + gq * 8 + jsel;
+        atomicAdd(r.env_acc + t, (double)y0);
+        atomicAdd(r.env_acc + r.HWpad + t, (double)y1);
+        atomicAdd(r.env_acc + 2 * r.HWpad + t, (double)y2);
+      }
+    }
+  }
+  float* red = s_red + warp * NACC * 32 + lane;
+  const float* av = &acc.Da0;
+#pragma unroll
+  for (int q = 0; q < NACC; ++q) red[q * 32] = av[q];
+  __syncthreads();
+  if (warp == 0 && valid) {
+    float sums[NACC];
+#pragma unroll
+    for (int q = 0; q < NACC; ++q) sums[q] = 0.f;
+    for (int w = 0; w < kNW; ++w)
+#pragma unroll
+      for (int q = 0; q < NACC; ++q) sums[q] += s_red[w * NACC * 32 + q * 32 + lane];
+    const BwdOutputs o{r.g_normal, r.g_view, r.g_albedo, r.g_spec, r.g_rough};
+    finish_bwd_point<DIFF, SPEC>(sums, g, sc, SPEC ? r.rough[pid] : 0.f, r.g_shading + 3 * pid, pid, o);
+  }
+}
+
+template <bool FWD>
+__device__ __forceinline__ void dispatch_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
+  const int key = (r.diff ? 4 : 0) | (r.spec ? 2 : 0) | (r.has_vis ? 1 : 0);
+  switch (key) {
+#define DES_TILE_CASE(K, D, S, V)                                       \
+  case K:                                                               \
+    if (FWD) fwd_tile<D, S, V>(r, tile, s_tab, s_red);                  \
+    else bwd_tile<D, S, V>(r, tile, s_tab, s_red);                      \
+    break;
+    DES_TILE_CASE(7, true, true, true)
+    DES_TILE_CASE(6, true, true, false)
+    DES_TILE_CASE(5, true, false, true)
+    DES_TILE_CASE(4, true, false, false)
+    DES_TILE_CASE(3, false, true, true)
+    DES_TILE_CASE(2, false, true, false)
+#undef DES_TILE_CASE
+    default:
+      break;
+  }
+}
+
+__global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __restrict__ reqs, WorkList* wl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* s_tab = reinterpret_cast<float4*>(smem_raw);
+  float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)kMaxHWpad * 32);
+  __shared__ int s_item[2];
+  __shared__ int s_last;
+  const unsigned n = wl->n;
+  int staged_req = -1;
+  const float4* staged_table = nullptr;
+  if (threadIdx.x == 0) s_item[0] = (int)atomicAdd(&wl->counter, 1u);
+  __syncthreads();
+  for (int it = 0;; ++it) {
+    const int idx = s_item[it & 1];
+    if (idx >= (int)n) break;
+    if (threadIdx.x == 0) s_item[(it + 1) & 1] = (int)atomicAdd(&wl->counter, 1u);
+    const WorkItem item = wl->items[idx];
+    // a malformed work item is reported and skipped, never dereferenced
+    if (item.req < 0 || item.req >= kMaxSlots || (item.kind != 0 && item.kind != 1) || item.tile < 0 ||
+        (int64_t)item.tile * 32 >= reqs[item.req < 0 || item.req >= kMaxSlots ? 0 : item.req].P) {
+      if (threadIdx.x == 0) atomicOr(&reqs[0].ctrl[kCtrlError], 4u);
+      __syncthreads();
+      continue;
+    }
+    const ReqDesc& r = reqs[item.req];
+    if (item.req != staged_req || r.table != staged_table) {
+      stage_table(s_tab, r.table, 0, r.HWpad);
+      staged_req = item.req;
+      staged_table = r.table;
+      __syncthreads();
+    }
+    if (item.kind == 0) {
+      dispatch_tile<true>(r, item.tile, s_tab, s_red);
+    } else {
+      dispatch_tile<false>(r, item.tile, s_tab, s_red);
+      // the CTA that finishes a request's last adjoint tile converts its FP64 env gradient
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicSub(r.bwd_tiles_left, 1u) == 1u) ? 1 : 0;
+      }
+      __syncthreads();
+      if (s_last) {
+        __threadfence();
+        for (int i = threadIdx.x; i < 3 * r.HW; i += blockDim.x) {
+          const int c = i / r.HW, t = i - c * r.HW;
+          r.g_env[i] = (float)r.env_acc[c * r.HWpad + t];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host: arena allocator, server
+// ---------------------------------------------------------------------------------------------
+
+// First-fit allocator over one device arena (offsets only; nothing is allocated per request).
+class Arena {
+ public:
+  void init(size_t bytes) {
+    free_.clear();
+    free_[0] = bytes;
+    total_ = bytes;
+  }
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = (bytes + 255) / 256 * 256;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= bytes) {
+        *off = it->first;
+        const size_t rest = it->second - bytes, start = it->first + bytes;
+        free_.erase(it);
+        if (rest) free_[start] = rest;
+        used_ += bytes;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = (bytes + 255) / 256 * 256;
+    used_ -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  size_t used() const { return used_; }
+  size_t total() const { return total_; }
+
+ private:
+  std::map<size_t, size_t> free_;
+  size_t total_ = 0, used_ = 0;
+};
+
+int64_t now_ns() {
+  return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+enum class State { Pending, Uploading, Ready, Downloading };
+
+struct Req {
+  int64_t ticket;
+  des_serve_request in;
+  State state = State::Pending;
+  int64_t t_submit = 0, t_admit = 0;
+  size_t off = 0, bytes = 0;
+  int slot = -1;
+  int n_tiles = 0;
+  int fwd_issued = 0, bwd_issued = 0, fwd_done = 0, bwd_done = 0;
+  double cost_fwd_tile = 0, cost_bwd_tile = 0;
+  ReqDesc desc{};
+  cudaEvent_t ev = nullptr;
+  // device pointers of outputs (for the download)
+  float *d_shading = nullptr, *d_white = nullptr, *d_gn = nullptr, *d_gv = nullptr, *d_ga = nullptr,
+        *d_gs = nullptr, *d_gr = nullptr, *d_genv = nullptr;
+  double remaining() const {
+    return (n_tiles - fwd_issued) * cost_fwd_tile + (in.backward ? (n_tiles - bwd_issued) * cost_bwd_tile : 0.0);
+  }
+};
+
+struct Env {
+  int H, W, HWpad;
+  float4* table;
+};
+struct Mesh {
+  int N_face, N_vertex, N_slot;
+  int32_t* faces;
+  uint32_t* vis;
+};
+
+struct Tick {
+  WorkList* h = nullptr;  // pinned
+  WorkList* d = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphNode_t copy_node = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool busy = false;
+  std::vector<std::pair<Req*, std::pair<int, int>>> counts;  // request, (fwd tiles, bwd tiles)
+};
+
+}  // namespace serve
+}  // namespace des
+
+struct des_server {
+  int device = 0;
+  int tick_us = 150;
+  double pairs_per_us = 0;  // throughput estimate used to size ticks
+  cudaStream_t copy = nullptr;
+  unsigned char* arena_base = nullptr;
+  des::serve::Arena arena;
+  unsigned* d_ctrl = nullptr;
+  des::serve::ReqDesc* d_reqs = nullptr;
+  des::serve::SlotStage* h_stage = nullptr;  // pinned staging for descriptor uploads (one per slot)
+  std::vector<int> free_slots;
+  std::vector<des::serve::Env> envs;
+  std::vector<des::serve::Mesh> meshes;
+  des::serve::Tick ticks[des::serve::kNTicks];
+  int sms = 0, grid = 0;
+  size_t smem = 0;
+
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<des::serve::Req*> incoming;
+  std::deque<des::serve::Req*> pending;
+  std::vector<des::serve::Req*> active;
+  std::vector<des_serve_done> completed;
+  int64_t next_ticket = 1;
+  int64_t n_submitted = 0, n_done = 0;
+  int error = DES_OK;
+  std::atomic<bool> stop{false};
+  std::thread worker;
+  int64_t t0 = 0;
+  des_serve_stats stats{};
+};
+
+namespace des {
+namespace serve {
+
+namespace {
+
+size_t request_bytes(const des_serve_request& q, int HWpad, int HW) {
+  const size_t P = (size_t)q.P;
+  size_t b = 0;
+  auto add = [&](size_t n) { b += (n + 255) / 256 * 256; };
+  add(P * 12 * 4);  // normal, view, albedo, specular albedo
+  add(P * 4);       // roughness
+  if (q.mesh_id >= 0) {
+    add(P * 8);
+    add(P * 12);
+  }
+  add(P * 12 * 2);  // shading, white
+  if (q.backward) {
+    add(P * 12 * 2);  // incoming gradients
+    add(P * 12 * 4 + P * 4);  // point gradients
+    add((size_t)3 * HWpad * 8);
+    add((size_t)3 * HW * 4);
+    add(256);
+  }
+  return b;
+}
+
+void upload(des_server* s, Req* r) {
+  const des_serve_request& q = r->in;
+  const Env& E = s->envs[q.env_id];
+  unsigned char* base = s->arena_base + r->off;
+  size_t off = 0;
+  auto take = [&](size_t n) {
+    unsigned char* p = base + off;
+    off += (n + 255) / 256 * 256;
+    return p;
+  };
+  const size_t P = (size_t)q.P;
+  ReqDesc& d = r->desc;
+  d = ReqDesc{};
+  d.P = q.P;
+  d.HW = E.H * E.W;
+  d.HWpad = E.HWpad;
+  d.diff = (q.flags & DES_DIFFUSE) ? 1 : 0;
+  d.spec = (q.flags & DES_SPECULAR) ? 1 : 0;
+  d.clamp = (q.flags & DES_CLAMP) != 0;
+  d.table = E.table;
+  d.ctrl = s->d_ctrl;
+  float* normal = (float*)take(P * 12);
+  float* view = (float*)take(P * 12);
+  float* albedo = (float*)take(P * 12);
+  float* spec = (float*)take(P * 12);
+  float* rough = (float*)take(P * 4);
+  cudaMemcpyAsync(normal, q.normal, P * 12, cudaMemcpyHostToDevice, s->copy);
+  cudaMemcpyAsync(view, q.view_dir, P * 12, cudaMemcpyHostToDevice, s->copy);
+  cudaMemcpyAsync(albedo, q.albedo, P * 12, cudaMemcpyHostToDevice, s->copy);
+  cudaMemcpyAsync(spec, q.specular_albedo, P * 12, cudaMemcpyHostToDevice, s->copy);
+  cudaMemcpyAsync(rough, q.roughness, P * 4, cudaMemcpyHostToDevice, s->copy);
+  d.normal = normal;
+  d.view = view;
+  d.albedo = albedo;
+  d.spec_alb = spec;
+  d.rough = rough;
+  if (q.mesh_id >= 0) {
+    const Mesh& M = s->meshes[q.mesh_id];
+    int64_t* tri = (int64_t*)take(P * 8);
+    float* bary = (float*)take(P * 12);
+    cudaMemcpyAsync(tri, q.nearest_triangle_id, P * 8, cudaMemcpyHostToDevice, s->copy);
+    cudaMemcpyAsync(bary, q.barycentric_coord, P * 12, cudaMemcpyHostToDevice, s->copy);
+    d.has_vis = 1;
+    d.N_face = M.N_face;
+    d.N_vertex = M.N_vertex;
+    d.faces = M.faces;
+    d.vis = M.vis;
+    d.tri = tri;
+    d.bary = bary;
+  }
+  r->d_shading = (float*)take(P * 12);
+  r->d_white = (float*)take(P * 12);
+  d.shading = r->d_shading;
+  d.white = r->d_white;
+  if (q.backward) {
+    float* gsh = (float*)take(P * 12);
+    float* gwh = (float*)take(P * 12);
+    cudaMemcpyAsync(gsh, q.grad_shading, P * 12, cudaMemcpyHostToDevice, s->copy);
+    if (q.grad_diffuse_shading) cudaMemcpyAsync(gwh, q.grad_diffuse_shading, P * 12, cudaMemcpyHostToDevice, s->copy);
+    d.g_shading = gsh;
+    d.g_white = q.grad_diffuse_shading ? gwh : nullptr;
+    unsigned char* g = take(P * 12 * 4 + P * 4);
+    r->d_gn = (float*)g;
+    r->d_gv = r->d_gn + 3 * P;
+    r->d_ga = r->d_gv + 3 * P;
+    r->d_gs = r->d_ga + 3 * P;
+    r->d_gr = r->d_gs + 3 * P;
+    d.g_normal = r->d_gn;
+    d.g_view = r->d_gv;
+    d.g_albedo = r->d_ga;
+    d.g_spec = r->d_gs;
+    d.g_rough = r->d_gr;
+    d.env_acc = (double*)take((size_t)3 * E.HWpad * 8);
+    r->d_genv = (float*)take((size_t)3 * d.HW * 4);
+    d.g_env = r->d_genv;
+    d.bwd_tiles_left = (unsigned*)take(256);
+    cudaMemsetAsync(d.env_acc, 0, (size_t)3 * E.HWpad * 8, s->copy);
+    s->h_stage[r->slot].tiles_left = (unsigned)r->n_tiles;
+    cudaMemcpyAsync(d.bwd_tiles_left, &s->h_stage[r->slot].tiles_left, sizeof(unsigned), cudaMemcpyHostToDevice,
+                    s->copy);
+  }
+  s->h_stage[r->slot].desc = d;
+  cudaMemcpyAsync(&s->d_reqs[r->slot], &s->h_stage[r->slot].desc, sizeof(ReqDesc), cudaMemcpyHostToDevice, s->copy);
+  cudaEventRecord(r->ev, s->copy);
+}
+
+void download(des_server* s, Req* r) {
+  const des_serve_request& q = r->in;
+  const size_t P = (size_t)q.P;
+  const Env& E = s->envs[q.env_id];
+  if (q.shading) cudaMemcpyAsync(q.shading, r->d_shading, P * 12, cudaMemcpyDeviceToHost, s->copy);
+  if (q.diffuse_shading) cudaMemcpyAsync(q.diffuse_shading, r->d_white, P * 12, cudaMemcpyDeviceToHost, s->copy);
+  if (q.backward) {
+    if (q.g_normal) cudaMemcpyAsync(q.g_normal, r->d_gn, P * 12, cudaMemcpyDeviceToHost, s->copy);
+    if (q.g_view_dir) cudaMemcpyAsync(q.g_view_dir, r->d_gv, P * 12, cudaMemcpyDeviceToHost, s->copy);
+    if (q.g_albedo) cudaMemcpyAsync(q.g_albedo, r->d_ga, P * 12, cudaMemcpyDeviceToHost, s->copy);
+    if (q.g_specular_albedo) cudaMemcpyAsync(q.g_specular_albedo, r->d_gs, P * 12, cudaMemcpyDeviceToHost, s->copy);
+    if (q.g_roughness) cudaMemcpyAsync(q.g_roughness, r->d_gr, P * 4, cudaMemcpyDeviceToHost, s->copy);
+    if (q.g_envmap)
+      cudaMemcpyAsync(q.g_envmap, r->d_genv, (size_t)3 * E.H * E.W * 4, cudaMemcpyDeviceToHost, s->copy);
+  }
+  cudaEventRecord(r->ev, s->copy);
+}
+
+// Builds and launches one tick if a tick buffer is free.  Returns true when work was launched.
+bool launch_tick(des_server* s) {
+  Tick* t = nullptr;
+  for (auto& k : s->ticks)
+    if (!k.busy) {
+      t = &k;
+      break;
+    }
+  if (t == nullptr) return false;
+  std::vector<Req*> ready;
+  for (Req* r : s->active)
+    if (r->state == State::Ready && r->remaining() > 0) ready.push_back(r);
+  if (ready.empty()) return false;
+  // shortest remaining work first; ties by arrival
+  std::stable_sort(ready.begin(), ready.end(), [](const Req* a, const Req* b) { return a->remaining() < b->remaining(); });
+  const double budget = s->pairs_per_us * s->tick_us;
+  double used = 0;
+  unsigned n = 0;
+  t->counts.clear();
+  for (Req* r : ready) {
+    if (used >= budget || n >= (unsigned)kTickItems) break;
+    int nf = 0, nb = 0;
+    while (used < budget && n < (unsigned)kTickItems && (r->fwd_issued < r->n_tiles ||
+                                                          (r->in.backward && r->bwd_issued < r->n_tiles))) {
+      // interleave forward and adjoint tiles of the same request
+      if (r->fwd_issued < r->n_tiles && (!r->in.backward || r->fwd_issued <= r->bwd_issued || r->bwd_issued >= r->n_tiles)) {
+        t->h->items[n++] = WorkItem{r->slot, r->fwd_issued++, 0, 0};
+        used += r->cost_fwd_tile;
+        ++nf;
+      } else {
+        t->h->items[n++] = WorkItem{r->slot, r->bwd_issued++, 1, 0};
+        used += r->cost_bwd_tile;
+        ++nb;
+      }
+    }
+    t->counts.push_back({r, {nf, nb}});
+  }
+  t->h->counter = 0;
+  t->h->n = n;
+  if (cudaGraphLaunch(t->exec, t->stream) != cudaSuccess) {
+    // launch the same work without the graph
+    cudaGetLastError();
+    cudaMemcpyAsync(t->d, t->h, sizeof(WorkList), cudaMemcpyHostToDevice, t->stream);
+    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_reqs, t->d);
+    s->stats.device_error |= 8;
+  }
+  cudaEventRecord(t->done, t->stream);
+  t->busy = true;
+  s->stats.ticks += 1;
+  s->stats.items += n;
+  return true;
+}
+
+void worker_loop(des_server* s) {
+  cudaSetDevice(s->device);
+  while (true) {
+    bool progressed = false;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      if (s->stop && s->incoming.empty() && s->pending.empty() && s->active.empty()) break;
+      while (!s->incoming.empty()) {
+        s->pending.push_back(s->incoming.front());
+        s->incoming.pop_front();
+      }
+    }
+    // 1. admission (arrival order; requests that do not fit yet are skipped, not blocking others)
+    for (auto it = s->pending.begin(); it != s->pending.end();) {
+      Req* r = *it;
+      const Env& E = s->envs[r->in.env_id];
+      r->bytes = request_bytes(r->in, E.HWpad, E.H * E.W);
+      size_t off = 0;
+      if (s->free_slots.empty() || !s->arena.alloc(r->bytes, &off)) {
+        ++it;
+        continue;
+      }
+      r->off = off;
+      r->slot = s->free_slots.back();
+      s->free_slots.pop_back();
+      r->t_admit = now_ns();
+      r->n_tiles = (int)((r->in.P + 31) / 32);
+      const double pairs = 32.0 * E.HWpad;
+      r->cost_fwd_tile = pairs;
+      r->cost_bwd_tile = 2.0 * pairs;
+      upload(s, r);
+      r->state = State::Uploading;
+      s->active.push_back(r);
+      it = s->pending.erase(it);
+      progressed = true;
+      s->stats.peak_arena_bytes = std::max<int64_t>(s->stats.peak_arena_bytes, (int64_t)s->arena.used());
+    }
+    // 2. finished ticks
+    for (auto& t : s->ticks) {
+      if (t.busy && cudaEventQuery(t.done) == cudaSuccess) {
+        for (auto& c : t.counts) {
+          c.first->fwd_done += c.second.first;
+          c.first->bwd_done += c.second.second;
+        }
+        t.counts.clear();
+        t.busy = false;
+        progressed = true;
+      }
+    }
+    // 3. request state transitions
+    for (auto it = s->active.begin(); it != s->active.end();) {
+      Req* r = *it;
+      if (r->state == State::Uploading && cudaEventQuery(r->ev) == cudaSuccess) {
+        r->state = State::Ready;
+        progressed = true;
+      }
+      if (r->state == State::Ready && r->fwd_done == r->n_tiles && (!r->in.backward || r->bwd_done == r->n_tiles)) {
+        download(s, r);
+        r->state = State::Downloading;
+        progressed = true;
+      }
+      if (r->state == State::Downloading && cudaEventQuery(r->ev) == cudaSuccess) {
+        des_serve_done d{};
+        d.ticket = r->ticket;
+        d.t_submit_ns = r->t_submit - s->t0;
+        d.t_admit_ns = r->t_admit - s->t0;
+        d.t_done_ns = now_ns() - s->t0;
+        d.status = DES_OK;
+        s->arena.release(r->off, r->bytes);
+        s->free_slots.push_back(r->slot);
+        cudaEventDestroy(r->ev);
+        {
+          std::lock_guard<std::mutex> lk(s->mu);
+          s->completed.push_back(d);
+          s->n_done += 1;
+        }
+        s->cv.notify_all();
+        delete r;
+        it = s->active.erase(it);
+        progressed = true;
+        continue;
+      }
+      ++it;
+    }
+    // 4. new ticks
+    while (launch_tick(s)) progressed = true;
+    if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(10));
+  }
+}
+
+}  // namespace
+}  // namespace serve
+}  // namespace des
+
+// ---------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------
+
+using des::serve::Req;
+
+extern "C" {
+
+int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_server** out) {
+  if (out == nullptr || hbm_budget_bytes < (1u << 20) || tick_us <= 0) return DES_ERR_INVALID_ARGUMENT;
+  auto* s = new des_server();
+  s->device = device;
+  s->tick_us = tick_us;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete s;
+    return DES_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
+  // a conservative starting throughput; it only sizes ticks
+  s->pairs_per_us = 1.5e5 * s->sms / 148.0;
+  bool ok = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&s->arena_base, hbm_budget_bytes) == cudaSuccess &&
+            cudaMalloc(&s->d_ctrl, 256) == cudaSuccess &&
+            cudaMalloc(&s->d_reqs, sizeof(des::serve::ReqDesc) * des::serve::kMaxSlots) == cudaSuccess &&
+            cudaMallocHost(&s->h_stage, sizeof(des::serve::SlotStage) * des::serve::kMaxSlots) == cudaSuccess &&
+            cudaMemset(s->d_ctrl, 0, 256) == cudaSuccess;
+  if (!ok) {
+    des_server_destroy(s);
+    return DES_ERR_CUDA;
+  }
+  s->arena.init(hbm_budget_bytes);
+  for (int i = des::serve::kMaxSlots - 1; i >= 0; --i) s->free_slots.push_back(i);
+  s->smem = (size_t)des::serve::kMaxHWpad * 32 + (size_t)des::serve::kNW * 15 * 32 * 4;
+  if (cudaFuncSetAttribute(des::serve::batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem) !=
+      cudaSuccess) {
+    des_server_destroy(s);
+    return DES_ERR_CUDA;
+  }
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, des::serve::batch_kernel, des::serve::kNW * 32, s->smem);
+  s->grid = std::max(1, occ) * s->sms;
+  // one captured graph per tick buffer: work-list upload + the persistent batch kernel
+  for (auto& t : s->ticks) {
+    ok = cudaMallocHost(&t.h, sizeof(des::serve::WorkList)) == cudaSuccess &&
+         cudaMalloc(&t.d, sizeof(des::serve::WorkList)) == cudaSuccess &&
+         cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+      des_server_destroy(s);
+      return DES_ERR_CUDA;
+    }
+    std::memset(t.h, 0, sizeof(des::serve::WorkList));
+    cudaMemset(t.d, 0, sizeof(des::serve::WorkList));
+    cudaGraph_t g = nullptr;
+    ok = cudaStreamBeginCapture(t.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    cudaMemcpyAsync(t.d, t.h, sizeof(des::serve::WorkList), cudaMemcpyHostToDevice, t.stream);
+    des::serve::batch_kernel<<<s->grid, des::serve::kNW * 32, s->smem, t.stream>>>(s->d_reqs, t.d);
+    ok = ok && cudaStreamEndCapture(t.stream, &g) == cudaSuccess;
+    size_t nn = 0;
+    ok = ok && cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn == 2;
+    cudaGraphNode_t nodes[2];
+    ok = ok && cudaGraphGetNodes(g, nodes, &nn) == cudaSuccess;
+    if (ok) {
+      cudaGraphNodeType ty;
+      cudaGraphNodeGetType(nodes[0], &ty);
+      t.copy_node = (ty == cudaGraphNodeTypeMemcpy) ? nodes[0] : nodes[1];
+      ok = cudaGraphInstantiate(&t.exec, g, 0) == cudaSuccess;
+    }
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+      des_server_destroy(s);
+      return DES_ERR_CUDA;
+    }
+  }
+  s->t0 = des::serve::now_ns();
+  s->worker = std::thread(des::serve::worker_loop, s);
+  *out = s;
+  return DES_OK;
+}
+
+int des_server_add_envmap(des_server* s, int32_t H, int32_t W, const float* envmap, const float* light2obj_rotmat,
+                          int32_t* env_id) {
+  if (s == nullptr || envmap == nullptr || light2obj_rotmat == nullptr || env_id == nullptr || H <= 0 || W <= 0)
+    return DES_ERR_INVALID_ARGUMENT;
+  const int HWpad = (H * W + 31) / 32 * 32;
+  if (HWpad > des::serve::kMaxHWpad) return DES_ERR_UNSUPPORTED;
+  cudaSetDevice(s->device);
+  float *d_env = nullptr, *d_R = nullptr;
+  des::serve::Env e{H, W, HWpad, nullptr};
+  unsigned* ctrl = nullptr;
+  bool ok = cudaMalloc(&d_env, sizeof(float) * 3 * H * W) == cudaSuccess && cudaMalloc(&d_R, 9 * 4) == cudaSuccess &&
+            cudaMalloc(&e.table, (size_t)HWpad * 32) == cudaSuccess && cudaMalloc(&ctrl, 256) == cudaSuccess &&
+            cudaMemcpy(d_env, envmap, sizeof(float) * 3 * H * W, cudaMemcpyDefault) == cudaSuccess &&
+            cudaMemcpy(d_R, light2obj_rotmat, 36, cudaMemcpyDefault) == cudaSuccess &&
+            des::launch_table(H, W, HWpad, d_R, d_env, e.table, ctrl, nullptr) == DES_OK &&
+            cudaDeviceSynchronize() == cudaSuccess;
+  cudaFree(d_env);
+  cudaFree(d_R);
+  cudaFree(ctrl);
+  if (!ok) return DES_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->envs.push_back(e);
+  *env_id = (int32_t)s->envs.size() - 1;
+  return DES_OK;
+}
+
+int des_server_add_mesh(des_server* s, int32_t N_face, int32_t N_vertex, int32_t N_slot,
+                        const int32_t* face_vertex_list, const int32_t* visibility, int32_t* mesh_id) {
+  if (s == nullptr || face_vertex_list == nullptr || visibility == nullptr || mesh_id == nullptr || N_face <= 0 ||
+      N_vertex <= 0 || N_slot <= 0)
+    return DES_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  des::serve::Mesh m{N_face, N_vertex, N_slot, nullptr, nullptr};
+  bool ok = cudaMalloc(&m.faces, (size_t)3 * N_face * 4) == cudaSuccess &&
+            cudaMalloc(&m.vis, (size_t)N_slot * N_vertex * 4) == cudaSuccess &&
+            cudaMemcpy(m.faces, face_vertex_list, (size_t)3 * N_face * 4, cudaMemcpyDefault) == cudaSuccess &&
+            cudaMemcpy(m.vis, visibility, (size_t)N_slot * N_vertex * 4, cudaMemcpyDefault) == cudaSuccess;
+  if (!ok) {
+    cudaFree(m.faces);
+    cudaFree(m.vis);
+    return DES_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->meshes.push_back(m);
+  *mesh_id = (int32_t)s->meshes.size() - 1;
+  return DES_OK;
+}
+
+int des_server_submit(des_server* s, const des_serve_request* req, int64_t* ticket) {
+  if (s == nullptr || req == nullptr || ticket == nullptr || req->P <= 0) return DES_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (req->env_id < 0 || req->env_id >= (int)s->envs.size()) return DES_ERR_INVALID_ARGUMENT;
+  if (req->mesh_id >= (int)s->meshes.size()) return DES_ERR_INVALID_ARGUMENT;
+  if (req->mesh_id >= 0) {
+    const auto& m = s->meshes[req->mesh_id];
+    const auto& e = s->envs[req->env_id];
+    if ((int64_t)m.N_slot * 32 < (int64_t)e.H * e.W || !req->nearest_triangle_id || !req->barycentric_coord)
+      return DES_ERR_INVALID_ARGUMENT;
+  }
+  if (!req->normal || !req->view_dir || !req->albedo || !req->specular_albedo || !req->roughness || !req->shading)
+    return DES_ERR_INVALID_ARGUMENT;
+  if (req->backward && !req->grad_shading) return DES_ERR_INVALID_ARGUMENT;
+  if (!(req->flags & (DES_DIFFUSE | DES_SPECULAR)) || (req->flags & ~(unsigned)(DES_DIFFUSE | DES_SPECULAR | DES_CLAMP)))
+    return DES_ERR_INVALID_ARGUMENT;
+  auto* r = new Req();
+  r->ticket = s->next_ticket++;
+  r->in = *req;
+  r->t_submit = des::serve::now_ns();
+  if (cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess) {
+    delete r;
+    return DES_ERR_CUDA;
+  }
+  s->incoming.push_back(r);
+  s->n_submitted += 1;
+  *ticket = r->ticket;
+  return DES_OK;
+}
+
+int des_server_poll(des_server* s, des_serve_done* out, int max_items, int* count) {
+  if (s == nullptr || count == nullptr || (max_items > 0 && out == nullptr)) return DES_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  const int n = std::min<int>(max_items, (int)s->completed.size());
+  for (int i = 0; i < n; ++i) out[i] = s->completed[i];
+  s->completed.erase(s->completed.begin(), s->completed.begin() + n);
+  *count = n;
+  return DES_OK;
+}
+
+int des_server_drain(des_server* s, int timeout_ms) {
+  if (s == nullptr) return DES_ERR_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  const bool done = s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms),
+                                   [&] { return s->n_done == s->n_submitted; });
+  return done ? DES_OK : DES_ERR_TIMEOUT;
+}
+
+int des_server_stats(des_server* s, des_serve_stats* out) {
+  if (s == nullptr || out == nullptr) return DES_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->stats;
+  out->submitted = s->n_submitted;
+  out->completed = s->n_done;
+  unsigned err = 0;
+  cudaMemcpy(&err, s->d_ctrl + des::kCtrlError, 4, cudaMemcpyDeviceToHost);
+  out->device_error = (int)err | s->stats.device_error;
+  return DES_OK;
+}
+
+int des_server_destroy(des_server* s) {
+  if (s == nullptr) return DES_ERR_INVALID_ARGUMENT;
+  if (s->worker.joinable()) {
+    s->stop = true;
+    s->worker.join();
+  }
+  cudaSetDevice(s->device);
+  cudaDeviceSynchronize();
+  for (auto& t : s->ticks) {
+    if (t.exec) cudaGraphExecDestroy(t.exec);
+    if (t.h) cudaFreeHost(t.h);
+    if (t.d) cudaFree(t.d);
+    if (t.done) cudaEventDestroy(t.done);
+    if (t.stream) cudaStreamDestroy(t.stream);
+  }
+  for (auto& e : s->envs) cudaFree(e.table);
+  for (auto& m : s->meshes) {
+    cudaFree(m.faces);
+    cudaFree(m.vis);
+  }
+  for (Req* r : s->pending) delete r;
+  for (Req* r : s->incoming) delete r;
+  if (s->h_stage) cudaFreeHost(s->h_stage);
+  if (s->d_reqs) cudaFree(s->d_reqs);
+  if (s->d_ctrl) cudaFree(s->d_ctrl);
+  if (s->arena_base) cudaFree(s->arena_base);
+  if (s->copy) cudaStreamDestroy(s->copy);
+  delete s;
+  return DES_OK;
+}
+
+}  // extern "C"

@@ -203,35 +203,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_fwd_kernel(const ShadePara
 // Backward (point gradients + env-map gradient in one pass)
 // ------------------------------------------------------------------------------------------
 
-// Transposing butterfly: e[j] (j = 0..7) per lane -> every lane holds the 32-lane sum of texel
-// 4*b4 + 2*b3 + b2 of its lane id (b4 = bit 4, ...), identical in lanes that differ in bits 0-1.
-__device__ __forceinline__ float butterfly8(const float (&e)[8], int lane) {
-  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
-  float x[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float keep = b4 ? e[i + 4] : e[i];
-    const float send = b4 ? e[i] : e[i + 4];
-    x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-  }
-  float y[2];
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const float keep = b3 ? x[i + 2] : x[i];
-    const float send = b3 ? x[i] : x[i + 2];
-    y[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-  }
-  float z;
-  {
-    const float keep = b2 ? y[1] : y[0];
-    const float send = b2 ? y[0] : y[1];
-    z = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-  }
-  z += __shfl_xor_sync(0xffffffffu, z, 2);
-  z += __shfl_xor_sync(0xffffffffu, z, 1);
-  return z;
-}
-
 template <bool DIFF, bool SPEC, bool VIS>
 __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadeParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -286,11 +257,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
     }
     if (SPEC) sc = spec_const(valid ? p.rough[pid] : 0.f, g);
 
-    float Da0 = 0.f, Da1 = 0.f, Da2 = 0.f;  // sum L * diffuse weight  -> g_albedo
-    float Sa0 = 0.f, Sa1 = 0.f, Sa2 = 0.f;  // sum L * specular weight -> g_specular_albedo
-    float gnx = 0.f, gny = 0.f, gnz = 0.f;
-    float gvx = 0.f, gvy = 0.f, gvz = 0.f;
-    float ga1 = 0.f, ga2 = 0.f, gbs = 0.f;  // d/d k, d/d alpha^2, sum of d/d b (G1 view factor)
+    BwdAcc acc = {};
+    const BwdPoint gp{gd0, gd1, gd2, gs0, gs1, gs2};
 
     for (int c = 0; c < nchunks; ++c) {
       const int cbase = c * p.chunk;
@@ -320,85 +288,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
           for (int j = 0; j < 8; ++j) {
             const float4 A = rec[2 * (gq * 8 + j)];
             const float4 B = rec[2 * (gq * 8 + j) + 1];
-            const float nl = dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z);
             const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
-            const bool act = nl > 0.f;
-            wdj[j] = 0.f;
-            wsj[j] = 0.f;
-            if (DIFF) {
-              // Lambert adjoint (bruteforce_shader.cu:2413-2426)
-              const float wdv = act ? B.w * vis : 0.f;  // d_omega/pi * vis
-              const float wd = nl * wdv;
-              Da0 = fmaf(B.x, wd, Da0);
-              Da1 = fmaf(B.y, wd, Da1);
-              Da2 = fmaf(B.z, wd, Da2);
-              const float gdot = dot3(gd0, gd1, gd2, B.x, B.y, B.z) * wdv;
-              gnx = fmaf(gdot, A.x, gnx);
-              gny = fmaf(gdot, A.y, gny);
-              gnz = fmaf(gdot, A.z, gnz);
-              wdj[j] = wd;
-            }
-            if (SPEC) {
-              const float hx = A.x + g.vx, hy = A.y + g.vy, hz = A.z + g.vz;
-              const float hh = fmaxf(dot3(hx, hy, hz, hx, hy, hz), kHalfVecFloor);
-              const float ri = rsqrt_approx(hh);
-              const float nh = dot3(g.nx, g.ny, g.nz, hx, hy, hz) * ri;
-              const float lh = dot3(A.x, A.y, A.z, hx, hy, hz) * ri;
-              const float a = 1.f - __saturatef(lh);
-              const float a2 = a * a;
-              const float a4 = a2 * a2;
-              const float F = fmaf(a4 * a, 1.f - kR0, kR0);
-              const float ia = rcp_approx(fmaf(nl, sc.omk, sc.k));
-              const float Ga = nl * ia;
-              const float G = Ga * sc.invB;
-              const float nh2 = nh * nh;
-              const float tt = ggx_t(g, hx, hy, hz, ri, nh2, sc);
-              const float t2 = kPiF * tt * tt;
-              const float itm = rcp_approx(fmaxf(t2, kThres));
-              const float D = sc.alpha2 * itm;
-              const float tmp = F * G * D * 0.25f;
-              const float wsv = (act && tmp > 0.f) ? A.w * vis : 0.f;  // d_omega * vis
-              const float ws = tmp * wsv;
-              Sa0 = fmaf(B.x, ws, Sa0);
-              Sa1 = fmaf(B.y, ws, Sa1);
-              Sa2 = fmaf(B.z, ws, Sa2);
-              wsj[j] = ws;
-              // d shading / d tmp, then split into F, G, D (bruteforce_shader.cu:2436-2445)
-              const float q = dot3(gs0, gs1, gs2, B.x, B.y, B.z) * wsv * 0.25f;
-              const float gF = q * (G * D);
-              const float gG = q * (F * D);
-              const float gD = q * (F * G);
-              // Fresnel adjoint (bruteforce_shader.cu:155-159)
-              const float gch = (lh >= 0.f && lh <= 1.f) ? (5.f * (kR0 - 1.f)) * gF * a4 : 0.f;
-              float ghx = gch * A.x, ghy = gch * A.y, ghz = gch * A.z;
-              // Schlick-Smith adjoint, light side (bruteforce_shader.cu:173-201); the view side is
-              // linear in a per-point factor and is applied once per point after the loop
-              const float gA = gG * sc.invB;
-              const float ia2 = ia * ia;
-              const float gdln = gA * sc.k * ia2;
-              gnx = fmaf(gdln, A.x, gnx);
-              gny = fmaf(gdln, A.y, gny);
-              gnz = fmaf(gdln, A.z, gnz);
-              ga1 = fmaf(gA * ia2, fmaf(nl, nl, -nl), ga1);
-              gbs = fmaf(-gA * Ga, sc.invB, gbs);
-              // GGX NDF adjoint (bruteforce_shader.cu:212-227); 1/t = pi t / (pi t^2)
-              ga2 = fmaf(gD, itm, ga2);
-              const float gt = (t2 > kThres) ? (-2.f * kPiF) * sc.alpha2 * gD * tt * itm * itm : 0.f;
-              ga2 = fmaf(nh2, gt, ga2);
-              const float gdnh = 2.f * gt * sc.am1 * nh;
-              const float hnx = hx * ri, hny = hy * ri, hnz = hz * ri;
-              gnx = fmaf(gdnh, hnx, gnx);
-              gny = fmaf(gdnh, hny, gny);
-              gnz = fmaf(gdnh, hnz, gnz);
-              ghx = fmaf(gdnh, g.nx, ghx);
-              ghy = fmaf(gdnh, g.ny, ghy);
-              ghz = fmaf(gdnh, g.nz, ghz);
-              // normalize adjoint (bruteforce_shader.cu:63-71) and h = l + v -> v
-              const float hg = dot3(hnx, hny, hnz, ghx, ghy, ghz);
-              gvx = fmaf(fmaf(-hnx, hg, ghx), ri, gvx);
-              gvy = fmaf(fmaf(-hny, hg, ghy), ri, gvy);
-              gvz = fmaf(fmaf(-hnz, hg, ghz), ri, gvz);
-            }
+            pair_bwd<DIFF, SPEC>(g, sc, gp, A, B, vis, acc, wdj[j], wsj[j]);
           }
           if (VIS) {
             w0 >>= 8;
@@ -430,61 +321,21 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
 
     // combine the NW texel ranges in warp order, then finish the per-point chain rule
     float* red = s_red + warp * NACC * 32 + lane;
-    red[0 * 32] = Da0; red[1 * 32] = Da1; red[2 * 32] = Da2;
-    red[3 * 32] = Sa0; red[4 * 32] = Sa1; red[5 * 32] = Sa2;
-    red[6 * 32] = gnx; red[7 * 32] = gny; red[8 * 32] = gnz;
-    red[9 * 32] = gvx; red[10 * 32] = gvy; red[11 * 32] = gvz;
-    red[12 * 32] = ga1; red[13 * 32] = ga2; red[14 * 32] = gbs;
+    const float* av = &acc.Da0;
+#pragma unroll
+    for (int q = 0; q < NACC; ++q) red[q * 32] = av[q];
     __syncthreads();
     if (warp == 0 && valid) {
-      float acc[NACC];
+      float sums[NACC];
 #pragma unroll
-      for (int q = 0; q < NACC; ++q) acc[q] = 0.f;
+      for (int q = 0; q < NACC; ++q) sums[q] = 0.f;
       for (int w = 0; w < NW; ++w) {
         const float* r = s_red + w * NACC * 32 + lane;
 #pragma unroll
-        for (int q = 0; q < NACC; ++q) acc[q] += r[q * 32];
+        for (int q = 0; q < NACC; ++q) sums[q] += r[q * 32];
       }
-      float n_x = acc[6], n_y = acc[7], n_z = acc[8];
-      float v_x = acc[9], v_y = acc[10], v_z = acc[11];
-      float g_rough = 0.f;
-      if (SPEC) {
-        // view side of the Schlick-Smith adjoint (bruteforce_shader.cu:194-200)
-        const float gdvn = acc[14] * sc.omk;
-        if (sc.nvp > 0.f) {
-          v_x = fmaf(gdvn, g.nx, v_x);
-          v_y = fmaf(gdvn, g.ny, v_y);
-          v_z = fmaf(gdvn, g.nz, v_z);
-          n_x = fmaf(gdvn, g.vx, n_x);
-          n_y = fmaf(gdvn, g.vy, n_y);
-          n_z = fmaf(gdvn, g.vz, n_z);
-        }
-        const float gk = fmaf(acc[14], 1.f - sc.nvp, acc[12]);
-        // roughness chain rule (bruteforce_shader.cu:2501-2502)
-        const float r = p.rough[pid];
-        g_rough = acc[13] * 4.f * r * r * r;
-        g_rough += gk * (1.f + r) / 4.f;
-      }
-      p.g_normal[3 * pid] = n_x;
-      p.g_normal[3 * pid + 1] = n_y;
-      p.g_normal[3 * pid + 2] = n_z;
-      const float g0 = p.g_shading[3 * pid], g1 = p.g_shading[3 * pid + 1], g2 = p.g_shading[3 * pid + 2];
-      if (p.g_albedo != nullptr) {
-        p.g_albedo[3 * pid] = DIFF ? g0 * acc[0] : 0.f;
-        p.g_albedo[3 * pid + 1] = DIFF ? g1 * acc[1] : 0.f;
-        p.g_albedo[3 * pid + 2] = DIFF ? g2 * acc[2] : 0.f;
-      }
-      if (p.g_spec != nullptr) {
-        p.g_spec[3 * pid] = SPEC ? g0 * acc[3] : 0.f;
-        p.g_spec[3 * pid + 1] = SPEC ? g1 * acc[4] : 0.f;
-        p.g_spec[3 * pid + 2] = SPEC ? g2 * acc[5] : 0.f;
-      }
-      if (p.g_view != nullptr) {
-        p.g_view[3 * pid] = SPEC ? v_x : 0.f;
-        p.g_view[3 * pid + 1] = SPEC ? v_y : 0.f;
-        p.g_view[3 * pid + 2] = SPEC ? v_z : 0.f;
-      }
-      if (p.g_rough != nullptr) p.g_rough[pid] = g_rough;
+      const BwdOutputs o{p.g_normal, p.g_view, p.g_albedo, p.g_spec, p.g_rough};
+      finish_bwd_point<DIFF, SPEC>(sums, g, sc, SPEC ? p.rough[pid] : 0.f, p.g_shading + 3 * pid, pid, o);
     }
     __syncthreads();
     tile = s_next[it & 1];

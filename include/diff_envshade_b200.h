@@ -127,6 +127,72 @@ size_t des_relight_workspace_bytes(int64_t P, int32_t H, int32_t W, int32_t K);
 int des_relight_multienv(const des_shade_args* args, const float* envmaps, int32_t K, unsigned flags, float* out,
                          void* workspace, size_t workspace_bytes, des_stream_t stream);
 
+/* ---------------------------------------------------------------------------------------
+ * Serving: continuous batching of shading requests (no reference counterpart; the reference
+ * is a per-call library, bruteforce_shader.cu:3261-3453 is its per-request path)
+ * ------------------------------------------------------------------------------------- */
+
+typedef struct des_server des_server;
+
+/* One request.  All pointers are host memory, pinned (cudaMallocHost / torch pin_memory) for
+ * asynchronous copies, and must stay valid until the request is reported done. */
+typedef struct des_serve_request {
+  int64_t P;
+  int32_t env_id;   /* from des_server_add_envmap */
+  int32_t mesh_id;  /* from des_server_add_mesh, or -1 for no visibility */
+  unsigned flags;   /* DES_DIFFUSE | DES_SPECULAR [| DES_CLAMP] */
+  int32_t backward; /* 0: shading only; 1: shading and all gradients */
+  const float* normal;
+  const float* view_dir;
+  const float* albedo;
+  const float* specular_albedo;
+  const float* roughness;
+  const int64_t* nearest_triangle_id; /* P, when mesh_id >= 0 */
+  const float* barycentric_coord;     /* 3 x P, when mesh_id >= 0 */
+  const float* grad_shading;          /* P x 3, when backward */
+  const float* grad_diffuse_shading;  /* P x 3 or NULL, when backward */
+  float* shading;                     /* P x 3 out */
+  float* diffuse_shading;             /* P x 3 out, or NULL */
+  float* g_normal;                    /* backward outputs (each may be NULL) */
+  float* g_view_dir;
+  float* g_albedo;
+  float* g_specular_albedo;
+  float* g_roughness;
+  float* g_envmap; /* 3 x H x W */
+} des_serve_request;
+
+typedef struct des_serve_done {
+  int64_t ticket;
+  int64_t t_submit_ns, t_admit_ns, t_done_ns; /* steady clock, relative to server creation */
+  int32_t status;
+  int32_t pad;
+} des_serve_done;
+
+typedef struct des_serve_stats {
+  int64_t submitted, completed, ticks, items, peak_arena_bytes;
+  int32_t device_error; /* workspace error word of the batch kernel (bit 0: bad mesh index) */
+  int32_t pad;
+} des_serve_stats;
+
+/* Starts a server on `device` with a device arena of hbm_budget_bytes (requests are admitted only
+ * while their buffers fit) and a scheduling tick of about tick_us microseconds of GPU work. */
+int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_server** out);
+/* Registers a resident env map (3 x H x W radiance and 3 x 3 rotation, host or device memory). */
+int des_server_add_envmap(des_server* s, int32_t H, int32_t W, const float* envmap, const float* light2obj_rotmat,
+                          int32_t* env_id);
+/* Registers a resident mesh: faces (3 x N_face) and visibility words (N_slot x N_vertex). */
+int des_server_add_mesh(des_server* s, int32_t N_face, int32_t N_vertex, int32_t N_slot,
+                        const int32_t* face_vertex_list, const int32_t* visibility, int32_t* mesh_id);
+/* Queues a request; returns immediately with its ticket. */
+int des_server_submit(des_server* s, const des_serve_request* req, int64_t* ticket);
+/* Moves up to max_items finished requests (outputs already in host memory) into out[]. */
+int des_server_poll(des_server* s, des_serve_done* out, int max_items, int* count);
+/* Waits until every submitted request has finished (DES_ERR_TIMEOUT after timeout_ms). */
+int des_server_drain(des_server* s, int timeout_ms);
+int des_server_stats(des_server* s, des_serve_stats* out);
+/* Finishes queued work and frees the server. */
+int des_server_destroy(des_server* s);
+
 /* The rotated texel table the kernels integrate over, written to table_out[H*W x 4] as
  * (x, y, z, d_omega) per texel in memory order.  Bit-exact with the reference's per-pair
  * getLightDir / getDeltaOmega / rotation (bruteforce_shader.cu:124-147, 2174-2197). */
