@@ -12,6 +12,10 @@ events).  Multi-GPU (torchrun): every rank shades its own 70k points (weak scali
 env-map gradients are summed over ranks with one NCCL all-reduce (the path's only exchange);
 the reported time is the max over ranks.
 
+At N = 1 the line also carries a serving leg ("serving"): 2000 requests (Poisson 5k/s, 1k-500k
+points, 16x32 or 32x64 env, visibility on/off, 30% with gradients) through the continuous-batching
+server against the same arrivals served one at a time by the plain operators (--no-serve skips it).
+
 ``--impl reference`` times the CPU restatement of the reference's sum (the reference has no
 CPU path of its own) on the host cores, on a bounded sample of the same workload.
 """
@@ -33,7 +37,9 @@ METRIC = "fwd+bwd point*texel/s (70k pts, 16x32 env, 512-bit visibility)"
 UNIT = "point*texel/s"
 CONFIG_NAME = "vis-70k"
 
-# Algorithmic FP32-pipe instructions per (point, texel) pair (FMA = 1), see DESIGN.md.
+# Algorithmic FP32-pipe instructions per (point, texel) pair with visibility (FMA = 1), with texel
+# tables and per-point constants hoisted: forward = visibility 8 + n.l 3 + Lambert 6 + GGX 40;
+# fused adjoint = recompute 45 + Lambert adjoint 12 + GGX adjoint 84 + env-map accumulation 7.
 INSTR_FWD_VIS = 57
 INSTR_BWD_VIS = 148
 FP32_LANES_PER_SM = 128
@@ -47,6 +53,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     return ap.parse_args()
 
 
@@ -248,6 +255,7 @@ def main():
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
+    launches0 = des.kernel_launches()
     for i in range(K):
         flush.fill_(float(i))
         ev[i][0].record()
@@ -261,6 +269,7 @@ def main():
         des.set_timing_events(0, 0)
         allreduce_env_grad(g[5])
         ev[i][1].record()
+    launches = des.kernel_launches() - launches0
     torch.cuda.synchronize()
     if pg is not None:
         pg.barrier()
@@ -347,6 +356,12 @@ def main():
                     "work": f"{INSTR_FWD_VIS} instr/pair"},
     }
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        # served p50/p99 against serial plain launches on one arrival schedule (2000 requests, Poisson 5k/s)
+        from diff_envshade_b200 import serve_workload
+        serving = serve_workload.run(n=2000, rate=5000.0, tick_us=150)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, desc, threads = cpu_port_throughput(inp_host, target_s=10.0)
@@ -361,11 +376,12 @@ def main():
                                    f"{d.visibility.shape[0] * 32}-bit visibility, specular on, fwd+bwd",
                        "points_per_rank": P, "texels": HW, "parallelism": f"dp{world}" if world > 1 else "single",
                        "l2": "256 MiB buffer rewritten between timed steps (outside the timed events)"},
-            "gpu_launches": 5 * K,
+            "gpu_launches": launches,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
+            "serving": serving,
             "fwd_ms": float(np.mean(fwd_ms)), "bwd_ms": float(np.mean(bwd_ms)),
         }
         print(json.dumps(line))

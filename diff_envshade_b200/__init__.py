@@ -37,6 +37,7 @@ from ._C import (  # noqa: E402,F401  reference operator surface
     texel_table,
     workspace_bytes,
     set_timing_events,
+    kernel_launches,
     relight_multienv,
 )
 from .autograd import (  # noqa: E402,F401

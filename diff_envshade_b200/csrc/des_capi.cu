@@ -19,7 +19,7 @@ int validate(const des_shade_args* a, unsigned flags, bool backward, const void*
   if (a->C != 3) return DES_ERR_UNSUPPORTED;
   if (a->P < 0 || a->H <= 0 || a->W <= 0) return DES_ERR_INVALID_ARGUMENT;
   if ((int64_t)a->H * a->W > kMaxTexels) return DES_ERR_UNSUPPORTED;
-  if (flags & ~(unsigned)(DES_DIFFUSE | DES_SPECULAR | DES_CLAMP)) return DES_ERR_INVALID_ARGUMENT;
+  if (flags & ~(unsigned)(DES_DIFFUSE | DES_SPECULAR | DES_CLAMP | DES_INPUT_ORDER)) return DES_ERR_INVALID_ARGUMENT;
   if (a->envmap == nullptr || a->light2obj_rotmat == nullptr) return DES_ERR_INVALID_ARGUMENT;
   if (a->P == 0) return DES_OK;
   if (a->normal == nullptr || out0 == nullptr) return DES_ERR_INVALID_ARGUMENT;
@@ -81,6 +81,10 @@ size_t des_shade_workspace_bytes(int64_t P, int32_t H, int32_t W, unsigned flags
   if (cudaGetDevice(&prev) != cudaSuccess) return 0;
   if (device != prev && cudaSetDevice(device) != cudaSuccess) return 0;
   des::LaunchPlan lp = des::plan_launch(P, H, W, backward != 0, device);
+  if (flags & DES_INPUT_ORDER) {
+    lp.sort = false;
+    lp.sort_chunks = 0;
+  }
   int grid = std::max(des::shade_grid(lp, flags, backward != 0, false), des::shade_grid(lp, flags, backward != 0, true));
   if (device != prev) cudaSetDevice(prev);
   if (grid <= 0) return 0;
@@ -152,6 +156,8 @@ int des_set_timing_events(void* start_event, void* stop_event) {
   des::set_timing_events(static_cast<cudaEvent_t>(start_event), static_cast<cudaEvent_t>(stop_event));
   return DES_OK;
 }
+
+unsigned long long des_kernel_launches(void) { return des::launches_so_far(); }
 
 int des_workspace_status(void* workspace, size_t workspace_bytes, int* status_out, des_stream_t stream) {
   if (workspace == nullptr || workspace_bytes < des::kCtrlBytes || status_out == nullptr)

@@ -11,6 +11,11 @@ namespace des {
 constexpr int kMaxThreads = 512;  // largest CTA of the shading kernels (16 warps)
 constexpr int kChunk = 2048;      // texels of the table staged in shared memory at once
 constexpr size_t kCtrlBytes = 256;
+// Normal-direction ordering of the points (calls with P >= kSortMinP): a stable counting sort by
+// the octahedral cell (32 x 32 cells, Morton order) of each normal, in chunks of kSortChunk points.
+constexpr int kSortBins = 1024;
+constexpr int kSortChunk = 1024;
+constexpr int64_t kSortMinP = 16384;
 
 // control words at the start of every workspace
 enum : int { kCtrlTileCounter = 0, kCtrlError = 1 };
@@ -29,6 +34,7 @@ struct ShadeParams {
   const int64_t* tri;
   const float* bary;
   const uint32_t* vis;
+  const int32_t* perm;   // optional: tile slot -> point index (normal-direction order)
   const float4* table;  // [HWpad][2] texel records
   bool clamp;
   bool env_in_smem;
@@ -50,6 +56,8 @@ struct ShadeParams {
 struct LaunchPlan {
   int HWpad, chunk, ntiles, nw;
   bool env_in_smem;
+  bool sort;        // order the points by normal direction first
+  int sort_chunks;  // ceil(P / kSortChunk) when sorting
   size_t smem;
   int sms, max_smem;
 };
@@ -81,6 +89,9 @@ int launch_texel_table(int H, int W, const float* R, float* out, des_stream_t st
 int launch_table(int H, int W, int HWpad, const float* R, const float* env, float4* rec, unsigned* ctrl,
                  cudaStream_t stream);
 void set_timing_events(cudaEvent_t start, cudaEvent_t stop);
+// Running count of kernel launches issued by this library (all streams and devices).
+void count_launches(int n);
+unsigned long long launches_so_far();
 size_t relight_workspace_bytes(int64_t P, int H, int W, int K);
 int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigned flags, float* out, void* ws,
                    size_t ws_bytes, cudaStream_t stream);

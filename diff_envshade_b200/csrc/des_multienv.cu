@@ -576,6 +576,7 @@ int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigne
       return DES_ERR_CUDA;
     k<<<grid, relight::kThreads, L.total, stream>>>(prm);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+    count_launches(2);
   }
   return DES_OK;
 }

@@ -189,7 +189,9 @@ __device__ __forceinline__ void pair_bwd(const PointGeom& g, const SpecConst& sc
     const float a2 = a * a;
     const float a4 = a2 * a2;
     const float F = fmaf(a4 * a, 1.f - kR0, kR0);
-    const float ia = rcp_approx(fmaf(nl, sc.omk, sc.k));
+    // max(n.l, 0) as in G1_robust: equal to n.l on every pair that contributes, and it keeps the
+    // denominator >= k on the others, whose products are masked by multiplying with zero
+    const float ia = rcp_approx(fmaf(fmaxf(nl, 0.f), sc.omk, sc.k));
     const float Ga = nl * ia;
     const float G = Ga * sc.invB;
     const float nh2 = nh * nh;

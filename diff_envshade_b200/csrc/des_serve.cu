@@ -633,6 +633,7 @@ bool launch_tick(des_server* s) {
     batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_reqs, t->d);
     s->stats.device_error |= 8;
   }
+  count_launches(1);
   cudaEventRecord(t->done, t->stream);
   t->busy = true;
   s->stats.ticks += 1;

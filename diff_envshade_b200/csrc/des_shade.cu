@@ -83,8 +83,127 @@ __global__ void des_table_kernel(int H, int W, int HWpad, const float* __restric
 }
 
 // ------------------------------------------------------------------------------------------
-// Shared pieces of the shading kernels
+// Normal-direction ordering
 // ------------------------------------------------------------------------------------------
+// A warp shades 32 points against the same texel at the same time.  When the 32 normals point
+// the same way, whole texels lie below every lane's horizon (n.l <= 0 for all 32 points: no
+// diffuse and no specular contribution) and are skipped by a warp vote.  Points are therefore
+// visited in the order of a stable counting sort by the octahedral cell of their normal (y is
+// the polar axis; 32 x 32 cells in Morton order so that neighbouring cells stay close).  Each
+// point's own arithmetic is unchanged, so per-point results do not depend on the order.
+
+// Morton spread of a 5-bit value: bit i -> bit 2i.
+__device__ __forceinline__ unsigned spread5(unsigned v) {
+  v = (v | (v << 4)) & 0x0F0Fu;
+  v = (v | (v << 2)) & 0x3333u;
+  v = (v | (v << 1)) & 0x5555u;
+  return v;
+}
+
+__device__ __forceinline__ int normal_key(const float* __restrict__ normal, int64_t p) {
+  const float x = normal[3 * p], y = normal[3 * p + 1], z = normal[3 * p + 2];
+  const float s = fabsf(x) + fabsf(y) + fabsf(z);
+  float u = 0.f, v = 0.f;
+  if (s > 0.f) {
+    u = x / s;
+    v = z / s;
+    if (y < 0.f) {  // fold the lower hemisphere onto the outer triangles of the square
+      const float fu = (1.f - fabsf(v)) * (u >= 0.f ? 1.f : -1.f);
+      const float fv = (1.f - fabsf(u)) * (v >= 0.f ? 1.f : -1.f);
+      u = fu;
+      v = fv;
+    }
+  }
+  // [-1, 1] -> cell 0..31 (NaN inputs land in cell 0: fmaxf returns the non-NaN operand)
+  const unsigned iu = (unsigned)fminf(fmaxf((u + 1.f) * 16.f, 0.f), 31.f);
+  const unsigned iv = (unsigned)fminf(fmaxf((v + 1.f) * 16.f, 0.f), 31.f);
+  return (int)(spread5(iu) | (spread5(iv) << 1));
+}
+
+// counts[c][k] = points of chunk c (kSortChunk points) whose normal falls in cell k; keys[p] = cell.
+__global__ void __launch_bounds__(256) des_sort_hist_kernel(const float* __restrict__ normal, int64_t P,
+                                                           unsigned* __restrict__ counts,
+                                                           uint16_t* __restrict__ keys) {
+  __shared__ unsigned h[kSortBins];
+  for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) h[i] = 0u;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kSortChunk;
+  for (int i = threadIdx.x; i < kSortChunk; i += blockDim.x) {
+    const int64_t p = base + i;
+    if (p < P) {
+      const int k = normal_key(normal, p);
+      keys[p] = (uint16_t)k;
+      atomicAdd(&h[k], 1u);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) counts[(size_t)blockIdx.x * kSortBins + i] = h[i];
+}
+
+// counts[c][k] <- points of cell k in chunks before c; counts[nchunks][k] <- points in cells before k.
+// Their sum is the first output position of chunk c's points in cell k (cells in order, chunks in
+// order within a cell).  One block of kSortBins threads; thread k owns cell k.
+__global__ void __launch_bounds__(kSortBins) des_sort_scan_kernel(unsigned* __restrict__ counts, int nchunks) {
+  __shared__ unsigned warp_tot[kSortBins / 32];
+  const int k = threadIdx.x, lane = k & 31, w = k >> 5;
+  unsigned run = 0;
+  for (int c0 = 0; c0 < nchunks; c0 += 16) {
+    unsigned v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = (c0 + j < nchunks) ? counts[(size_t)(c0 + j) * kSortBins + k] : 0u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      if (c0 + j < nchunks) counts[(size_t)(c0 + j) * kSortBins + k] = run;
+      run += v[j];
+    }
+  }
+  // exclusive scan of the cell totals across the block
+  unsigned incl = run;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += t;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    unsigned x = warp_tot[lane];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= off) x += t;
+    }
+    warp_tot[lane] = x;  // inclusive over warps
+  }
+  __syncthreads();
+  counts[(size_t)nchunks * kSortBins + k] = (incl - run) + (w > 0 ? warp_tot[w - 1] : 0u);
+}
+
+// Stable scatter: one warp per chunk walks its points in input order, 32 at a time; lanes with the
+// same cell rank themselves with __match_any_sync and the lowest such lane advances the cursor.
+__global__ void __launch_bounds__(32) des_sort_scatter_kernel(const uint16_t* __restrict__ keys, int64_t P,
+                                                             const unsigned* __restrict__ counts,
+                                                             int32_t* __restrict__ perm) {
+  __shared__ unsigned cursor[kSortBins];
+  __shared__ uint16_t s_key[kSortChunk];
+  const int lane = threadIdx.x;
+  const int64_t base = (int64_t)blockIdx.x * kSortChunk;
+  const unsigned* cell_base = counts + (size_t)gridDim.x * kSortBins;
+  for (int i = lane; i < kSortBins; i += 32) cursor[i] = counts[(size_t)blockIdx.x * kSortBins + i] + cell_base[i];
+  for (int i = lane; i < kSortChunk; i += 32) s_key[i] = (base + i < P) ? keys[base + i] : (uint16_t)0;
+  __syncwarp();
+  const unsigned lt = (1u << lane) - 1u;
+  for (int r = 0; r < kSortChunk / 32; ++r) {
+    const int64_t p = base + r * 32 + lane;
+    const bool valid = p < P;
+    const int key = valid ? (int)s_key[r * 32 + lane] : kSortBins + lane;  // invalid lanes match no one
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (valid) perm[cursor[key] + __popc(peers & lt)] = (int32_t)p;
+    __syncwarp();
+    if (valid && (peers & lt) == 0u) cursor[key] += __popc(peers);
+    __syncwarp();
+  }
+}
 
 
 // ------------------------------------------------------------------------------------------
@@ -113,8 +232,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_fwd_kernel(const ShadePara
   while (tile < p.ntiles) {
     if (threadIdx.x == 0) s_next[it & 1] = (int)gridDim.x + (int)atomicAdd(&p.ctrl[kCtrlTileCounter], 1u);
 
-    const int64_t pid = (int64_t)tile * 32 + lane;
-    const bool valid = pid < p.P;
+    const int64_t slot = (int64_t)tile * 32 + lane;
+    const bool valid = slot < p.P;
+    const int64_t pid = (valid && p.perm != nullptr) ? (int64_t)p.perm[slot] : slot;
     const PointGeom g = load_geom<VIS>(p, pid, valid, need_view);
     SpecConst sc;
     if (SPEC) sc = spec_const(valid ? p.rough[pid] : 0.f, g);
@@ -148,6 +268,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_fwd_kernel(const ShadePara
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const float4 A = rec[2 * (gq * 8 + j)];
+            // texel below the horizon of all 32 points: it adds nothing to any of them
+            if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) continue;
             const float4 B = rec[2 * (gq * 8 + j) + 1];
             const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
             float wd, ws;
@@ -231,8 +353,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
   while (tile < p.ntiles) {
     if (threadIdx.x == 0) s_next[it & 1] = (int)gridDim.x + (int)atomicAdd(&p.ctrl[kCtrlTileCounter], 1u);
 
-    const int64_t pid = (int64_t)tile * 32 + lane;
-    const bool valid = pid < p.P;
+    const int64_t slot = (int64_t)tile * 32 + lane;
+    const bool valid = slot < p.P;
+    const int64_t pid = (valid && p.perm != nullptr) ? (int64_t)p.perm[slot] : slot;
     const PointGeom g = load_geom<VIS>(p, pid, valid, need_view);
     // incoming gradients folded with the albedos (bruteforce_shader.cu:2585-2588)
     float gd0 = 0.f, gd1 = 0.f, gd2 = 0.f, gs0 = 0.f, gs1 = 0.f, gs2 = 0.f;
@@ -284,9 +407,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
 #pragma unroll 1
         for (int gq = 0; gq < 4; ++gq) {
           float wdj[8], wsj[8];
+          bool live = false;  // warp-uniform: some texel of the group is above some lane's horizon
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
+            wdj[j] = 0.f;
+            wsj[j] = 0.f;
             const float4 A = rec[2 * (gq * 8 + j)];
+            // texel below the horizon of all 32 points: no contribution to any output
+            if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) continue;
+            live = true;
             const float4 B = rec[2 * (gq * 8 + j) + 1];
             const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
             pair_bwd<DIFF, SPEC>(g, sc, gp, A, B, vis, acc, wdj[j], wsj[j]);
@@ -296,6 +425,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
             w1 >>= 8;
             w2 >>= 8;
           }
+          if (!live) continue;
           // env-map gradient of these 8 texels: per lane e = gd * wd + gs * ws, summed over lanes
           const int t0 = ebase + (sl << 5) + gq * 8;
           const int jsel = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
@@ -471,6 +601,8 @@ LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev) {
   lp.smem = (size_t)lp.chunk * 32 + (lp.env_in_smem ? (size_t)lp.chunk * 24 : 0) + (size_t)nw * nacc * 32 * 4;
   lp.sms = di.sms;
   lp.max_smem = di.max_smem_optin;
+  lp.sort = P >= kSortMinP;
+  lp.sort_chunks = lp.sort ? (int)((P + kSortChunk - 1) / kSortChunk) : 0;
   return lp;
 }
 
@@ -478,6 +610,11 @@ size_t workspace_bytes(const LaunchPlan& lp, bool backward, int grid) {
   size_t off = kCtrlBytes;
   off += align_up((size_t)lp.HWpad * 32, 256);  // texel table
   if (backward) off += align_up((size_t)std::max(grid, 1) * 3 * lp.HWpad * sizeof(double), 256);
+  if (lp.sort) {
+    off += align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256);                    // permutation
+    off += align_up((size_t)(lp.sort_chunks + 1) * kSortBins * sizeof(unsigned), 256);  // cell offsets
+    off += align_up((size_t)lp.ntiles * 32 * sizeof(uint16_t), 256);                   // cell of each point
+  }
   return off;
 }
 
@@ -501,6 +638,13 @@ void set_timing_events(cudaEvent_t start, cudaEvent_t stop) {
   g_timing_stop.store(stop);
 }
 
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
+
+void count_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+unsigned long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
+
 int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   const des_shade_args& a = *call.args;
@@ -509,10 +653,21 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return DES_ERR_CUDA;
   LaunchPlan lp = plan_launch(a.P, a.H, a.W, call.backward, dev);
+  if (call.flags & DES_INPUT_ORDER) {
+    lp.sort = false;
+    lp.sort_chunks = 0;
+  }
   if (lp.smem > (size_t)lp.max_smem) return DES_ERR_UNSUPPORTED;
   const int grid = shade_grid(lp, call.flags, call.backward, vis);
   if (grid <= 0) return DES_ERR_CUDA;
-  const size_t need = workspace_bytes(lp, call.backward, grid);
+  size_t need = workspace_bytes(lp, call.backward, grid);
+  if (lp.sort && call.workspace_bytes < need) {
+    // a workspace sized for input order (e.g. the allocation-free entry point's static array):
+    // shade in input order -- same results, no ordering scratch
+    lp.sort = false;
+    lp.sort_chunks = 0;
+    need = workspace_bytes(lp, call.backward, grid);
+  }
   if (call.workspace == nullptr || call.workspace_bytes < need ||
       (reinterpret_cast<uintptr_t>(call.workspace) & 255u) != 0)
     return DES_ERR_WORKSPACE;
@@ -521,6 +676,15 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   unsigned* ctrl = reinterpret_cast<unsigned*>(ws);
   float4* table = reinterpret_cast<float4*>(ws + kCtrlBytes);
   double* env_partial = reinterpret_cast<double*>(ws + kCtrlBytes + align_up((size_t)lp.HWpad * 32, 256));
+  unsigned char* sort_area =
+      ws + kCtrlBytes + align_up((size_t)lp.HWpad * 32, 256) +
+      (call.backward ? align_up((size_t)std::max(grid, 1) * 3 * lp.HWpad * sizeof(double), 256) : 0);
+  int32_t* perm = reinterpret_cast<int32_t*>(sort_area);
+  unsigned* sort_counts =
+      reinterpret_cast<unsigned*>(sort_area + align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256));
+  uint16_t* sort_keys = reinterpret_cast<uint16_t*>(
+      reinterpret_cast<unsigned char*>(sort_counts) +
+      align_up((size_t)(lp.sort_chunks + 1) * kSortBins * sizeof(unsigned), 256));
 
   // texel table + control-word reset
   {
@@ -529,6 +693,7 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
     des_table_kernel<<<blocks, threads, 0, stream>>>(a.H, a.W, lp.HWpad, a.light2obj_rotmat, a.envmap, table,
                                                      nullptr, ctrl);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+    count_launches(1);
   }
   if (a.P == 0) {
     if (call.backward && call.g_envmap != nullptr)
@@ -584,12 +749,22 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   prm.g_rough = call.g_rough;
   prm.env_partial = env_partial;
   prm.env_in_smem = lp.env_in_smem;
+  prm.perm = nullptr;
+  if (lp.sort) {
+    des_sort_hist_kernel<<<lp.sort_chunks, 256, 0, stream>>>(a.normal, a.P, sort_counts, sort_keys);
+    des_sort_scan_kernel<<<1, kSortBins, 0, stream>>>(sort_counts, lp.sort_chunks);
+    des_sort_scatter_kernel<<<lp.sort_chunks, 32, 0, stream>>>(sort_keys, a.P, sort_counts, perm);
+    if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+    count_launches(3);
+    prm.perm = perm;
+  }
 
   KernelFn k = call.backward ? pick<BwdSel>(diff, spec, vis) : pick<FwdSel>(diff, spec, vis);
   cudaEvent_t ev0 = g_timing_start.load(), ev1 = g_timing_stop.load();
   if (ev0 != nullptr && ev1 != nullptr) cudaEventRecord(ev0, stream);
   k<<<grid, lp.nw * 32, lp.smem, stream>>>(prm);
   if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+  count_launches(1);
   if (ev0 != nullptr && ev1 != nullptr) cudaEventRecord(ev1, stream);
 
   if (call.backward && call.g_envmap != nullptr) {
@@ -597,6 +772,7 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
     const int rg = (3 * lp.HWpad + 31) / 32;
     des_env_reduce_kernel<<<rg, rb, 0, stream>>>(env_partial, grid, a.H * a.W, lp.HWpad, call.g_envmap);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+    count_launches(1);
   }
   return DES_OK;
 }
@@ -605,6 +781,7 @@ int launch_table(int H, int W, int HWpad, const float* R, const float* env, floa
                  cudaStream_t stream) {
   const int threads = 256;
   des_table_kernel<<<(HWpad + threads - 1) / threads, threads, 0, stream>>>(H, W, HWpad, R, env, rec, nullptr, ctrl);
+  count_launches(1);
   return cudaGetLastError() == cudaSuccess ? DES_OK : DES_ERR_CUDA;
 }
 
@@ -614,6 +791,7 @@ int launch_texel_table(int H, int W, const float* R, float* out, des_stream_t st
   const int threads = 256;
   des_table_kernel<<<(HWpad + threads - 1) / threads, threads, 0, stream>>>(H, W, HWpad, R, nullptr, nullptr, out,
                                                                             nullptr);
+  count_launches(1);
   return cudaGetLastError() == cudaSuccess ? DES_OK : DES_ERR_CUDA;
 }
 

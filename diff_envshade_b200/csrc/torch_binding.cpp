@@ -428,6 +428,8 @@ Tensor texel_table(int64_t H, int64_t W, const Tensor& R) {
 
 // Times the main kernel of subsequent shading calls with the caller's CUDA events (raw handles,
 // e.g. torch.cuda.Event().cuda_event); pass 0, 0 to stop.
+int64_t kernel_launches() { return static_cast<int64_t>(des_kernel_launches()); }
+
 void set_timing_events(int64_t start, int64_t stop) {
   des_set_timing_events(reinterpret_cast<void*>(start), reinterpret_cast<void*>(stop));
 }
@@ -458,6 +460,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         py::arg("visibility") = py::none(), py::arg("enable_specular") = true, py::arg("split") = true);
   m.def("workspace_bytes", &workspace_bytes, "scratch bytes of one shading call");
   m.def("set_timing_events", &set_timing_events, "bracket the main kernel of later calls with these CUDA events");
+  m.def("kernel_launches", &kernel_launches, "kernels launched by the native library so far");
   m.attr("DES_DIFFUSE") = (int)DES_DIFFUSE;
   m.attr("DES_SPECULAR") = (int)DES_SPECULAR;
   m.attr("DES_CLAMP") = (int)DES_CLAMP;

@@ -94,11 +94,24 @@ def pack_bits(bits):
     """bits: bool [P, n_texels] -> int32 [ceil(n/32), P] words, texel t = bit t%32 of slot t//32."""
     P, n = bits.shape
     nslots = (n + 31) // 32
-    b = np.zeros((P, nslots * 32), dtype=np.uint64)
-    b[:, :n] = bits.numpy().astype(np.uint64)
-    b = b.reshape(P, nslots, 32)
-    words = (b << np.arange(32, dtype=np.uint64)).sum(axis=2).astype(np.uint32)  # [P, nslots]
+    b = bits.numpy()
+    if n != nslots * 32:
+        b = np.concatenate([b, np.zeros((P, nslots * 32 - n), dtype=bool)], axis=1)
+    # little-endian bit order within each byte and byte order within each word: bit t%32 of word t//32
+    words = np.packbits(b, axis=1, bitorder="little").view("<u4")  # [P, nslots]
     return torch.from_numpy(np.ascontiguousarray(words.T).view(np.int32))
+
+
+def random_visibility(g, N_vertex, n_texels, p, rows_per_draw=None):
+    """Packed Bernoulli(p) visibility words [ceil(n/32), N_vertex].  Large tables are drawn in blocks
+    of vertices so that host memory stays bounded; tables of up to 2^28 bits are one draw."""
+    if rows_per_draw is None:
+        rows_per_draw = N_vertex if N_vertex * n_texels <= (1 << 28) else max(1, (1 << 25) // n_texels)
+    parts = []
+    for v0 in range(0, N_vertex, rows_per_draw):
+        rows = min(rows_per_draw, N_vertex - v0)
+        parts.append(pack_bits(torch.rand(rows, n_texels, generator=g) < p))
+    return parts[0] if len(parts) == 1 else torch.cat(parts, dim=1).contiguous()
 
 
 def unpack_bits(words, n_texels):
@@ -140,11 +153,10 @@ def make_inputs(P, H, W, seed, sigma=1.0, rough=(0.2, 0.9), vis_p=None, vis_layo
             bary = (e / e.sum(0, keepdim=True)).contiguous()
         else:
             raise ValueError(vis_layout)
-        bits = torch.rand(N_vertex, HW, generator=g) < vis_p
         inp.face_vertex_list = faces.contiguous()
         inp.nearest_triangle_id = tri.contiguous()
         inp.barycentric_coord = bary.contiguous()
-        inp.visibility = pack_bits(bits)
+        inp.visibility = random_visibility(g, N_vertex, HW, vis_p)
     if grads:
         inp.grad_shading = torch.randn(P, 3, generator=g)
         inp.grad_diffuse_shading = torch.randn(P, 3, generator=g)

@@ -44,6 +44,12 @@ typedef enum des_status {
 #define DES_SPECULAR 2u /* GGX term (Schlick Fresnel, Schlick-Smith G, GGX NDF)          */
 #define DES_CLAMP 4u    /* backface clamp: a point with n.v <= 0 shades to zero          */
 #define DES_RELIGHT_BF16 8u /* des_relight_multienv: plain BF16 operands (default: BF16 hi+lo split) */
+/* des_shade_*: shade the points in input order.  By default calls with P >= 16384 first order the
+ * points by the octahedral cell of their normal, so that a warp's 32 points face the same way and
+ * texels below all of their horizons are skipped.  The outputs are the same either way (per-point
+ * values bit for bit; the env-map gradient up to FP64 summation order).  Input order needs a
+ * smaller workspace; a workspace too small for the ordering also falls back to input order. */
+#define DES_INPUT_ORDER 16u
 
 /* All inputs of one shading call.  The visibility block is ignored when visibility == NULL. */
 typedef struct des_shade_args {
@@ -102,7 +108,8 @@ int des_shade_backward(const des_shade_args* args, unsigned flags, const float* 
  * reference).  Same inputs and outputs as des_shade_backward, no workspace argument: scratch comes
  * from a library-owned static device array of DES_SHADE_NOALLOC_SCRATCH_BYTES, held on every GPU
  * that uses it until the process exits.  Returns DES_ERR_WORKSPACE, without launching anything,
- * when des_shade_workspace_bytes(P, H, W, flags, 1, device) exceeds that size.  All calls share the
+ * when des_shade_workspace_bytes(P, H, W, flags | DES_INPUT_ORDER, 1, device) exceeds that size
+ * (a problem that fits only in input order runs in input order).  All calls share the
  * array: calls whose work overlaps on the GPU race and corrupt each other.  The first call on each
  * device looks up the array's address (cudaGetSymbolAddress); make it before any stream capture.
  * Allocates nothing. */
@@ -203,6 +210,11 @@ int des_texel_table(int32_t H, int32_t W, const float* light2obj_rotmat, float* 
  * fused adjoint) and `stop_event` immediately after it, so the caller can time that kernel alone.
  * Process-wide; pass NULL, NULL to turn it off. */
 int des_set_timing_events(void* start_event, void* stop_event);
+
+/* Number of kernels this library has launched since it was loaded, on every stream and device
+ * (a served tick counts once, whether it ran as a CUDA graph or as a plain launch).  Read it
+ * before and after a region to count the launches inside it. */
+unsigned long long des_kernel_launches(void);
 
 /* Copies the device-side error word of a workspace used by a finished call to *status_out
  * (DES_OK or DES_ERR_BAD_INDEX) and clears it.  Synchronises `stream`. */

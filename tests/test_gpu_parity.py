@@ -278,3 +278,43 @@ def test_cabi_direct_matches_torch_ops(des):
     st = ctypes.c_int(-1)
     assert L.des_workspace_status(cabi.ptr(ws), wsb, ctypes.byref(st), stream) == cabi.DES_OK
     assert st.value == cabi.DES_OK
+
+
+@pytest.mark.parametrize("P,layout", [(70000, "identity"), (40000, "mesh"), (16384, None)])
+def test_point_ordering_changes_no_result(des, P, layout):
+    """Calls with P >= 16384 shade the points ordered by normal direction and skip texels below all
+    32 lanes' horizons; DES_INPUT_ORDER turns that off.  Per-point outputs must be bit-identical
+    (each point's arithmetic is the same and a skipped texel adds exact zeros); the env-map
+    gradient differs only in FP64 summation order (gradient bound of conftest.py)."""
+    from diff_envshade_b200 import workloads as wl
+    inp = wl.make_inputs(P, 16, 32, seed=P + 3, vis_p=0.7 if layout else None, vis_layout=layout or "identity",
+                         rotation=True)
+    d = _dev(inp)
+    L = cabi.lib()
+    args = cabi.make_args(d)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    dev = torch.cuda.current_device()
+    res = {}
+    for order in (0, cabi.DES_INPUT_ORDER):
+        flags = cabi.DES_DIFFUSE | cabi.DES_SPECULAR | order
+        wsf = L.des_shade_workspace_bytes(args.P, args.H, args.W, flags, 0, dev)
+        wsb = L.des_shade_workspace_bytes(args.P, args.H, args.W, flags, 1, dev)
+        ws = torch.empty(max(wsf, wsb), dtype=torch.uint8, device="cuda")
+        sh, wh = torch.empty(P, 3, device="cuda"), torch.empty(P, 3, device="cuda")
+        assert L.des_shade_forward(ctypes.byref(args), flags, cabi.ptr(sh), cabi.ptr(wh), cabi.ptr(ws), wsf,
+                                   stream) == cabi.DES_OK
+        outs = [torch.empty(P, 3, device="cuda") for _ in range(4)] + [torch.empty(P, 1, device="cuda"),
+                                                                        torch.empty(3, 16, 32, device="cuda")]
+        assert L.des_shade_backward(ctypes.byref(args), flags, cabi.ptr(d.grad_shading),
+                                    cabi.ptr(d.grad_diffuse_shading), *[cabi.ptr(o) for o in outs], cabi.ptr(ws),
+                                    wsb, stream) == cabi.DES_OK
+        res[order] = [sh, wh] + outs
+    both = cabi.DES_DIFFUSE | cabi.DES_SPECULAR
+    assert L.des_shade_workspace_bytes(args.P, args.H, args.W, both, 1, dev) > \
+        L.des_shade_workspace_bytes(args.P, args.H, args.W, both | cabi.DES_INPUT_ORDER, 1, dev)
+    torch.cuda.synchronize()
+    for name, a, b in zip(("shading", "diffuse_shading") + GRAD_KEYS, res[0], res[cabi.DES_INPUT_ORDER]):
+        if name == "g_env":
+            assert_close_grad(a.cpu(), b.cpu(), "ordered-vs-input:g_env")
+        else:
+            assert torch.equal(a, b), f"ordered and input order differ in {name}"

@@ -2,8 +2,8 @@
 
 Both sides shade the same seeded inputs; forward + backward are timed with CUDA events after
 warm-up (median of 20 runs; a 256 MiB buffer is rewritten between runs so neither side starts
-from a warm L2).  The north-star bar for the 70,000-point, 16x32, 512-bit-visibility workload is
-at least 3x the reference's fwd+bwd time.  Set DES_PERF_OUT=<file> to also write the numbers as
+from a warm L2).  The bar for the 70,000-point, 16x32, 512-bit-visibility workload and for the
+1,048,576-point, 32x64, 2048-bit-visibility workload is at least 3x the reference's fwd+bwd time.  Set DES_PERF_OUT=<file> to also write the numbers as
 JSON.
 """
 import json
@@ -46,7 +46,8 @@ def _ops(mod, d, vis):
     return fwd, bwd
 
 
-@pytest.mark.parametrize("name,vis,min_speedup", [("vis-70k", True, 3.0), ("plain-4k", False, 1.0)])
+@pytest.mark.parametrize("name,vis,min_speedup", [("vis-70k", True, 3.0), ("plain-4k", False, 1.0),
+                                                    ("vis-1m", True, 3.0)])
 def test_faster_than_reference_kernels(reference_ext, name, vis, min_speedup):
     import diff_envshade_b200 as des
     from diff_envshade_b200 import workloads as wl

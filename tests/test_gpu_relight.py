@@ -2,7 +2,7 @@
 of the plain FP32 forward kernel.
 
 Tolerance: BF16 hi+lo split mode -- per element |d| <= 1e-3 (|ref| + 1e-3 max|ref|) against the FP64
-oracle (the north-star bound for this form); plain BF16 mode -- the same check at 2e-2, with its
+oracle (the accuracy bound set for the BF16 form); plain BF16 mode -- the same check at 2e-2, with its
 measured error printed.  Set DES_PERF_OUT=<file> to append the measured errors and timings as JSON.
 """
 import json

@@ -120,6 +120,19 @@ def test_visibility_pack_roundtrip_and_bit_order():
     one[0, 37] = True
     w = wl.pack_bits(one).numpy().view(np.uint32)
     assert w[1, 0] == 1 << 5 and w[0, 0] == 0
+    top = torch.zeros(1, 32, dtype=torch.bool)
+    top[0, 31] = True
+    assert wl.pack_bits(top).numpy().view(np.uint32)[0, 0] == 1 << 31
+
+
+def test_random_visibility_block_draws():
+    """Large tables are drawn in vertex blocks: same layout as one draw, Bernoulli(p) density."""
+    import torch
+    v = wl.random_visibility(torch.Generator().manual_seed(1), 1000, 100, 0.6, rows_per_draw=64)
+    assert v.shape == (4, 1000) and v.dtype == torch.int32
+    bits = wl.unpack_bits(v, 100)
+    assert abs(bits.float().mean().item() - 0.6) < 0.01
+    assert not wl.unpack_bits(v, 128)[:, 100:].any()  # padding bits of the last slot stay clear
 
 
 def test_identity_visibility_masks_texels():
