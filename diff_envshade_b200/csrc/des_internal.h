@@ -14,8 +14,11 @@ constexpr size_t kCtrlBytes = 256;
 // Normal-direction ordering of the points (calls with P >= kSortMinP): a stable counting sort by
 // the octahedral cell (32 x 32 cells, Morton order) of each normal, in chunks of kSortChunk points.
 constexpr int kSortBins = 1024;
-constexpr int kSortChunk = 1024;
+constexpr int kSortThreads = 512;       // threads of a ranking CTA (16 warps, 64 points each per pass)
+constexpr int kSortMinChunk = 1024;     // points ranked by one CTA: the smallest power-of-two
+constexpr int kSortMaxChunks = 128;     //   multiple of 1024 that needs at most 128 CTAs
 constexpr int64_t kSortMinP = 16384;
+constexpr int64_t kSortMaxP = int64_t(1) << 24;  // per-warp 16-bit cell counters stay below 2^16
 
 // control words at the start of every workspace
 enum : int { kCtrlTileCounter = 0, kCtrlError = 1 };
@@ -57,7 +60,8 @@ struct LaunchPlan {
   int HWpad, chunk, ntiles, nw;
   bool env_in_smem;
   bool sort;        // order the points by normal direction first
-  int sort_chunks;  // ceil(P / kSortChunk) when sorting
+  int sort_chunk;   // points per ranking CTA
+  int sort_chunks;  // ceil(P / sort_chunk) when sorting
   size_t smem;
   int sms, max_smem;
 };

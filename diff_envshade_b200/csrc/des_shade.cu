@@ -43,19 +43,12 @@ namespace des {
 // Texel table
 // ------------------------------------------------------------------------------------------
 
-// One launch per call: rec[2t] = (l'x, l'y, l'z, d_omega), rec[2t+1] = (L0, L1, L2, d_omega/pi)
-// for t < H*W, zeros for the padding up to a multiple of 32.  Also resets the control words of
-// the workspace (tile counter, error word) for the kernel that follows on the same stream.
-// `export4` (optional) receives (x, y, z, d_omega) per texel for des_texel_table.
-__global__ void des_table_kernel(int H, int W, int HWpad, const float* __restrict__ R,
-                                 const float* __restrict__ env, float4* __restrict__ rec,
-                                 float* __restrict__ export4, unsigned* __restrict__ ctrl) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t == 0 && ctrl != nullptr) {
-    ctrl[kCtrlTileCounter] = 0u;
-    ctrl[kCtrlError] = 0u;
-  }
-  if (t >= HWpad) return;
+// Texel record t: rec[2t] = (l'x, l'y, l'z, d_omega), rec[2t+1] = (L0, L1, L2, d_omega/pi) for
+// t < H*W, zeros for the padding up to a multiple of 32.  `export4` (optional) receives
+// (x, y, z, d_omega) per texel for des_texel_table.
+__device__ __forceinline__ void table_entry(int t, int H, int W, const float* __restrict__ R,
+                                            const float* __restrict__ env, float4* __restrict__ rec,
+                                            float* __restrict__ export4) {
   const int HW = H * W;
   if (t < HW) {
     int ix = t % W;
@@ -82,6 +75,19 @@ __global__ void des_table_kernel(int H, int W, int HWpad, const float* __restric
   }
 }
 
+// The texel table of one call (one thread per texel); also resets the control words of the
+// workspace (tile counter, error word) for the kernel that follows on the same stream.
+__global__ void des_table_kernel(int H, int W, int HWpad, const float* __restrict__ R,
+                                 const float* __restrict__ env, float4* __restrict__ rec,
+                                 float* __restrict__ export4, unsigned* __restrict__ ctrl) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0 && ctrl != nullptr) {
+    ctrl[kCtrlTileCounter] = 0u;
+    ctrl[kCtrlError] = 0u;
+  }
+  if (t < HWpad) table_entry(t, H, W, R, env, rec, export4);
+}
+
 // ------------------------------------------------------------------------------------------
 // Normal-direction ordering
 // ------------------------------------------------------------------------------------------
@@ -105,8 +111,9 @@ __device__ __forceinline__ int normal_key(const float* __restrict__ normal, int6
   const float s = fabsf(x) + fabsf(y) + fabsf(z);
   float u = 0.f, v = 0.f;
   if (s > 0.f) {
-    u = x / s;
-    v = z / s;
+    const float is = 1.f / s;
+    u = x * is;
+    v = z * is;
     if (y < 0.f) {  // fold the lower hemisphere onto the outer triangles of the square
       const float fu = (1.f - fabsf(v)) * (u >= 0.f ? 1.f : -1.f);
       const float fv = (1.f - fabsf(u)) * (v >= 0.f ? 1.f : -1.f);
@@ -120,91 +127,159 @@ __device__ __forceinline__ int normal_key(const float* __restrict__ normal, int6
   return (int)(spread5(iu) | (spread5(iv) << 1));
 }
 
-// counts[c][k] = points of chunk c (kSortChunk points) whose normal falls in cell k; keys[p] = cell.
-__global__ void __launch_bounds__(256) des_sort_hist_kernel(const float* __restrict__ normal, int64_t P,
-                                                           unsigned* __restrict__ counts,
-                                                           uint16_t* __restrict__ keys) {
-  __shared__ unsigned h[kSortBins];
-  for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) h[i] = 0u;
+// Ordering, step 1 (fused with the texel table and the control-word reset of the call).
+// CTA c ranks the points of chunk c = [c*chunk, (c+1)*chunk) (chunk a multiple of 1024), 1024
+// points at a time: warp w takes 64 consecutive points in 2 rounds of 32, and lanes with equal
+// cells rank themselves with __match_any_sync against the warp's own per-cell counters.  An
+// exclusive prefix of those counters over the warps then gives every point its rank among the
+// chunk's points of its cell (input order when the chunk is one pass of 1024 points; otherwise
+// warp by warp -- a fixed order either way, so the permutation is deterministic).  Outputs: keys[p] = cell, rank[p] = rank, and the chunk's cell
+// counts in column c of counts[k][ncp] (row length ncp = nchunks rounded up to 4).
+// Threads of every CTA also build the texel records (grid-stride over the table).
+__global__ void __launch_bounds__(kSortThreads, 1) des_prep_kernel(int H, int W, int HWpad, const float* __restrict__ R,
+                                                                const float* __restrict__ env,
+                                                                float4* __restrict__ rec, unsigned* __restrict__ ctrl,
+                                                                const float* __restrict__ normal, int64_t P,
+                                                                int chunk, int ncp, unsigned* __restrict__ counts,
+                                                                uint16_t* __restrict__ keys,
+                                                                uint32_t* __restrict__ rank) {
+  constexpr int NW = kSortThreads / 32;
+  constexpr int SUB = 2 * kSortThreads;  // points per pass: 2 rounds per warp
+  __shared__ uint16_t cnt[NW][kSortBins];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (blockIdx.x == 0 && tid == 0) {
+    ctrl[kCtrlTileCounter] = 0u;
+    ctrl[kCtrlError] = 0u;
+  }
+  for (int t = blockIdx.x * kSortThreads + tid; t < HWpad; t += gridDim.x * kSortThreads)
+    table_entry(t, H, W, R, env, rec, nullptr);
+
+  for (int i = tid; i < NW * kSortBins / 2; i += kSortThreads) reinterpret_cast<uint32_t*>(&cnt[0][0])[i] = 0u;
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * kSortChunk;
-  for (int i = threadIdx.x; i < kSortChunk; i += blockDim.x) {
-    const int64_t p = base + i;
-    if (p < P) {
-      const int k = normal_key(normal, p);
-      keys[p] = (uint16_t)k;
-      atomicAdd(&h[k], 1u);
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t cbase = (int64_t)blockIdx.x * chunk;
+  const int nsub = chunk / SUB;
+  int key[2] = {0, 0};
+  unsigned lr[2] = {0u, 0u};
+  for (int sub = 0; sub < nsub; ++sub) {
+    const int64_t wbase = cbase + (int64_t)sub * SUB + w * 64;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int64_t p = wbase + r * 32 + lane;
+      key[r] = (p < P) ? normal_key(normal, p) : kSortBins + lane;  // invalid lanes match no one
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int64_t p = wbase + r * 32 + lane;
+      const bool valid = p < P;
+      const unsigned peers = __match_any_sync(0xffffffffu, key[r]);
+      lr[r] = valid ? cnt[w][key[r]] + __popc(peers & lt) : 0u;
+      __syncwarp();
+      if (valid && (peers & lt) == 0u) cnt[w][key[r]] += (uint16_t)__popc(peers);
+      __syncwarp();
+      if (nsub > 1 && valid) {  // kept in registers when there is a single pass
+        keys[p] = (uint16_t)key[r];
+        rank[p] = lr[r];
+      }
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) counts[(size_t)blockIdx.x * kSortBins + i] = h[i];
+  // exclusive prefix of the per-warp counters over the warps, per cell; chunk totals to global
+  for (int k = tid; k < kSortBins; k += kSortThreads) {
+    unsigned run = 0;
+#pragma unroll
+    for (int q = 0; q < NW; ++q) {
+      const unsigned c = cnt[q][k];
+      cnt[q][k] = (uint16_t)run;
+      run += c;
+    }
+    counts[(size_t)k * ncp + blockIdx.x] = run;
+  }
+  __syncthreads();
+  if (nsub == 1) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int64_t p = cbase + w * 64 + r * 32 + lane;
+      if (p < P) {
+        keys[p] = (uint16_t)key[r];
+        rank[p] = cnt[w][key[r]] + lr[r];
+      }
+    }
+  } else {
+    for (int sub = 0; sub < nsub; ++sub) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int64_t p = cbase + (int64_t)sub * SUB + w * 64 + r * 32 + lane;
+        if (p < P) rank[p] += cnt[w][keys[p]];  // this thread wrote both in the first pass
+      }
+    }
+  }
 }
 
-// counts[c][k] <- points of cell k in chunks before c; counts[nchunks][k] <- points in cells before k.
-// Their sum is the first output position of chunk c's points in cell k (cells in order, chunks in
-// order within a cell).  One block of kSortBins threads; thread k owns cell k.
-__global__ void __launch_bounds__(kSortBins) des_sort_scan_kernel(unsigned* __restrict__ counts, int nchunks) {
+// Ordering, step 2.  CTA c: thread k reads row k of counts (cell k's count in every chunk) and
+// sums it over all chunks (total) and over the chunks before c (prefix); a block scan of the
+// totals gives the first position of cell k; then every point p of chunk c goes to
+// perm[first(k) + prefix_c(k) + rank[p]]: cells in order, chunks in order within a cell.
+__global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chunk, int nchunks, int ncp,
+                                                              const unsigned* __restrict__ counts,
+                                                              const uint16_t* __restrict__ keys,
+                                                              const uint32_t* __restrict__ rank,
+                                                              int32_t* __restrict__ perm) {
+  __shared__ unsigned off[kSortBins];
   __shared__ unsigned warp_tot[kSortBins / 32];
   const int k = threadIdx.x, lane = k & 31, w = k >> 5;
-  unsigned run = 0;
-  for (int c0 = 0; c0 < nchunks; c0 += 16) {
-    unsigned v[16];
+  const int c = blockIdx.x;
+  const uint4* row = reinterpret_cast<const uint4*>(counts + (size_t)k * ncp);
+  unsigned pre = 0, tot = 0;
+  for (int q0 = 0; q0 < ncp / 4; q0 += 8) {
+    uint4 v[8];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = (c0 + j < nchunks) ? counts[(size_t)(c0 + j) * kSortBins + k] : 0u;
+    for (int j = 0; j < 8; ++j) v[j] = (q0 + j < ncp / 4) ? row[q0 + j] : make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      if (c0 + j < nchunks) counts[(size_t)(c0 + j) * kSortBins + k] = run;
-      run += v[j];
+    for (int j = 0; j < 8; ++j) {
+      const int c0 = 4 * (q0 + j);  // columns from nchunks on are padding (never written)
+      tot += (c0 < nchunks ? v[j].x : 0u) + (c0 + 1 < nchunks ? v[j].y : 0u) + (c0 + 2 < nchunks ? v[j].z : 0u) +
+             (c0 + 3 < nchunks ? v[j].w : 0u);
+      pre += (c0 < c ? v[j].x : 0u) + (c0 + 1 < c ? v[j].y : 0u) + (c0 + 2 < c ? v[j].z : 0u) +
+             (c0 + 3 < c ? v[j].w : 0u);
     }
   }
-  // exclusive scan of the cell totals across the block
-  unsigned incl = run;
+  unsigned incl = tot;
 #pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const unsigned t = __shfl_up_sync(0xffffffffu, incl, off);
-    if (lane >= off) incl += t;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
   }
   if (lane == 31) warp_tot[w] = incl;
   __syncthreads();
   if (w == 0) {
     unsigned x = warp_tot[lane];
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const unsigned t = __shfl_up_sync(0xffffffffu, x, off);
-      if (lane >= off) x += t;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
     }
-    warp_tot[lane] = x;  // inclusive over warps
+    warp_tot[lane] = x;
   }
   __syncthreads();
-  counts[(size_t)nchunks * kSortBins + k] = (incl - run) + (w > 0 ? warp_tot[w - 1] : 0u);
-}
-
-// Stable scatter: one warp per chunk walks its points in input order, 32 at a time; lanes with the
-// same cell rank themselves with __match_any_sync and the lowest such lane advances the cursor.
-__global__ void __launch_bounds__(32) des_sort_scatter_kernel(const uint16_t* __restrict__ keys, int64_t P,
-                                                             const unsigned* __restrict__ counts,
-                                                             int32_t* __restrict__ perm) {
-  __shared__ unsigned cursor[kSortBins];
-  __shared__ uint16_t s_key[kSortChunk];
-  const int lane = threadIdx.x;
-  const int64_t base = (int64_t)blockIdx.x * kSortChunk;
-  const unsigned* cell_base = counts + (size_t)gridDim.x * kSortBins;
-  for (int i = lane; i < kSortBins; i += 32) cursor[i] = counts[(size_t)blockIdx.x * kSortBins + i] + cell_base[i];
-  for (int i = lane; i < kSortChunk; i += 32) s_key[i] = (base + i < P) ? keys[base + i] : (uint16_t)0;
-  __syncwarp();
-  const unsigned lt = (1u << lane) - 1u;
-  for (int r = 0; r < kSortChunk / 32; ++r) {
-    const int64_t p = base + r * 32 + lane;
-    const bool valid = p < P;
-    const int key = valid ? (int)s_key[r * 32 + lane] : kSortBins + lane;  // invalid lanes match no one
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
-    if (valid) perm[cursor[key] + __popc(peers & lt)] = (int32_t)p;
-    __syncwarp();
-    if (valid && (peers & lt) == 0u) cursor[key] += __popc(peers);
-    __syncwarp();
+  off[k] = (incl - tot) + (w > 0 ? warp_tot[w - 1] : 0u) + pre;
+  __syncthreads();
+  const int64_t base = (int64_t)c * chunk;
+  for (int i0 = 0; i0 < chunk; i0 += 4 * kSortBins) {
+    int kk[4];
+    unsigned rr[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t p = base + i0 + j * kSortBins + k;
+      const bool ok = (i0 + j * kSortBins < chunk) && p < P;
+      kk[j] = ok ? (int)keys[p] : -1;
+      rr[j] = ok ? rank[p] : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (kk[j] >= 0) perm[off[kk[j]] + rr[j]] = (int32_t)(base + i0 + j * kSortBins + k);
   }
 }
-
 
 // ------------------------------------------------------------------------------------------
 // Forward
@@ -581,6 +656,8 @@ struct BwdSel {
 };
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+// Row length of the [cell][chunk] count table: chunks rounded up to a multiple of 4 (16-byte rows).
+inline int sort_row(const LaunchPlan& lp) { return (lp.sort_chunks + 3) / 4 * 4; }
 
 }  // namespace
 
@@ -601,8 +678,10 @@ LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev) {
   lp.smem = (size_t)lp.chunk * 32 + (lp.env_in_smem ? (size_t)lp.chunk * 24 : 0) + (size_t)nw * nacc * 32 * 4;
   lp.sms = di.sms;
   lp.max_smem = di.max_smem_optin;
-  lp.sort = P >= kSortMinP;
-  lp.sort_chunks = lp.sort ? (int)((P + kSortChunk - 1) / kSortChunk) : 0;
+  lp.sort = P >= kSortMinP && P <= kSortMaxP;
+  lp.sort_chunk = kSortMinChunk;
+  while ((int64_t)lp.sort_chunk * kSortMaxChunks < P) lp.sort_chunk *= 2;
+  lp.sort_chunks = lp.sort ? (int)((P + lp.sort_chunk - 1) / lp.sort_chunk) : 0;
   return lp;
 }
 
@@ -611,9 +690,10 @@ size_t workspace_bytes(const LaunchPlan& lp, bool backward, int grid) {
   off += align_up((size_t)lp.HWpad * 32, 256);  // texel table
   if (backward) off += align_up((size_t)std::max(grid, 1) * 3 * lp.HWpad * sizeof(double), 256);
   if (lp.sort) {
-    off += align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256);                    // permutation
-    off += align_up((size_t)(lp.sort_chunks + 1) * kSortBins * sizeof(unsigned), 256);  // cell offsets
-    off += align_up((size_t)lp.ntiles * 32 * sizeof(uint16_t), 256);                   // cell of each point
+    off += align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256);                 // permutation
+    off += align_up((size_t)kSortBins * sort_row(lp) * sizeof(unsigned), 256);      // cell counts [cell][chunk]
+    off += align_up((size_t)lp.ntiles * 32 * sizeof(uint16_t), 256);                // cell of each point
+    off += align_up((size_t)lp.ntiles * 32 * sizeof(uint32_t), 256);                // rank of each point
   }
   return off;
 }
@@ -682,19 +762,25 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   int32_t* perm = reinterpret_cast<int32_t*>(sort_area);
   unsigned* sort_counts =
       reinterpret_cast<unsigned*>(sort_area + align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256));
-  uint16_t* sort_keys = reinterpret_cast<uint16_t*>(
-      reinterpret_cast<unsigned char*>(sort_counts) +
-      align_up((size_t)(lp.sort_chunks + 1) * kSortBins * sizeof(unsigned), 256));
+  uint16_t* sort_keys = reinterpret_cast<uint16_t*>(reinterpret_cast<unsigned char*>(sort_counts) +
+                                                    align_up((size_t)kSortBins * sort_row(lp) * sizeof(unsigned), 256));
+  uint32_t* sort_rank = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(sort_keys) +
+                                                    align_up((size_t)lp.ntiles * 32 * sizeof(uint16_t), 256));
 
-  // texel table + control-word reset
-  {
+  // texel table + control-word reset (+ step 1 of the ordering when ordering)
+  const bool sort = lp.sort && a.P > 0 && (diff || spec);
+  if (sort) {
+    des_prep_kernel<<<lp.sort_chunks, kSortThreads, 0, stream>>>(a.H, a.W, lp.HWpad, a.light2obj_rotmat, a.envmap,
+                                                                 table, ctrl, a.normal, a.P, lp.sort_chunk,
+                                                                 sort_row(lp), sort_counts, sort_keys, sort_rank);
+  } else {
     const int threads = 256;
     const int blocks = (lp.HWpad + threads - 1) / threads;
     des_table_kernel<<<blocks, threads, 0, stream>>>(a.H, a.W, lp.HWpad, a.light2obj_rotmat, a.envmap, table,
                                                      nullptr, ctrl);
-    if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
-    count_launches(1);
   }
+  if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+  count_launches(1);
   if (a.P == 0) {
     if (call.backward && call.g_envmap != nullptr)
       if (cudaMemsetAsync(call.g_envmap, 0, sizeof(float) * 3 * (size_t)a.H * a.W, stream) != cudaSuccess)
@@ -750,12 +836,11 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   prm.env_partial = env_partial;
   prm.env_in_smem = lp.env_in_smem;
   prm.perm = nullptr;
-  if (lp.sort) {
-    des_sort_hist_kernel<<<lp.sort_chunks, 256, 0, stream>>>(a.normal, a.P, sort_counts, sort_keys);
-    des_sort_scan_kernel<<<1, kSortBins, 0, stream>>>(sort_counts, lp.sort_chunks);
-    des_sort_scatter_kernel<<<lp.sort_chunks, 32, 0, stream>>>(sort_keys, a.P, sort_counts, perm);
+  if (sort) {
+    des_place_kernel<<<lp.sort_chunks, kSortBins, 0, stream>>>(a.P, lp.sort_chunk, lp.sort_chunks, sort_row(lp),
+                                                               sort_counts, sort_keys, sort_rank, perm);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
-    count_launches(3);
+    count_launches(1);
     prm.perm = perm;
   }
 

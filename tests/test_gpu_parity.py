@@ -280,10 +280,11 @@ def test_cabi_direct_matches_torch_ops(des):
     assert st.value == cabi.DES_OK
 
 
-@pytest.mark.parametrize("P,layout", [(70000, "identity"), (40000, "mesh"), (16384, None)])
+@pytest.mark.parametrize("P,layout", [(70000, "identity"), (40000, "mesh"), (16384, None), (300001, "identity")])
 def test_point_ordering_changes_no_result(des, P, layout):
     """Calls with P >= 16384 shade the points ordered by normal direction and skip texels below all
-    32 lanes' horizons; DES_INPUT_ORDER turns that off.  Per-point outputs must be bit-identical
+    32 lanes' horizons; DES_INPUT_ORDER turns that off.  (300,001 points: 4096-point ranking chunks
+    of several passes and a ragged last chunk.)  Per-point outputs must be bit-identical
     (each point's arithmetic is the same and a skipped texel adds exact zeros); the env-map
     gradient differs only in FP64 summation order (gradient bound of conftest.py)."""
     from diff_envshade_b200 import workloads as wl
