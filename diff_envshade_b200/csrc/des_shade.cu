@@ -3,7 +3,8 @@
 // Work decomposition (all shading kernels):
 //  * a tile is 32 consecutive points, one point per lane of a warp;
 //  * a CTA of NW warps processes one tile at a time, warp w integrating the tile over its own
-//    contiguous run of 32-texel visibility slots, so the NW warps split the texel axis;
+//    share of the 32-texel visibility slots (mirrored pairs, see warp_slot), so the NW warps
+//    split the texel axis;
 //  * CTAs are persistent: the grid is sized to the resident capacity of the device, and CTAs
 //    pull tiles from a device counter (the next tile index is fetched one tile ahead);
 //  * the texel table {rotated direction, d_omega, radiance, d_omega/pi} of the whole env map is
@@ -282,11 +283,27 @@ __global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chu
 }
 
 // ------------------------------------------------------------------------------------------
+// Texel split between the warps of a tile
+// ------------------------------------------------------------------------------------------
+// The k-th 32-texel slot (of nsl) integrated by warp `warp` of NW, or -1 past its last.  The
+// slots are taken in the order 0, nsl-1, 1, nsl-2, ... -- mirrored pairs, i.e. rows at opposite
+// elevations for the usual map widths -- and dealt to the warps a pair at a time (unit 2), or a
+// slot at a time when there are fewer pairs than warps (unit 1).  The horizon skip removes whole
+// rows for points that face up or down; mirrored pairs keep the surviving work of the warps of a
+// tile even, so they reach the end-of-tile barrier together.
+__device__ __forceinline__ int warp_slot(int k, int warp, int NW, int nsl, int ushift) {
+  // ushift = log2(unit)
+  const int j = (((k >> ushift) * NW + warp) << ushift) + (k & ushift);
+  if (j >= nsl) return -1;
+  return (j & 1) ? nsl - 1 - (j >> 1) : (j >> 1);
+}
+
+// ------------------------------------------------------------------------------------------
 // Forward
 // ------------------------------------------------------------------------------------------
 
 template <bool DIFF, bool SPEC, bool VIS>
-__global__ void __launch_bounds__(kMaxThreads, 1) des_fwd_kernel(const ShadeParams p) {
+__global__ void __maxnreg__(80) des_fwd_kernel(const ShadeParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* s_tab = reinterpret_cast<float4*>(smem_raw);
   float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)p.chunk * 32);
@@ -326,18 +343,21 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_fwd_kernel(const ShadePara
         __syncthreads();
       }
       const int nsl = clen >> 5;
-      const int sl0 = (warp * nsl) / NW, sl1 = ((warp + 1) * nsl) / NW;
+      const int ushift = ((nsl + 1) >> 1) >= NW ? 1 : 0;
       const int gslot0 = cbase >> 5;
       uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
-      if (VIS && sl0 < sl1) load_vis_words(p, g, valid, gslot0 + sl0, n0, n1, n2);
-      for (int sl = sl0; sl < sl1; ++sl) {
+      int sl = warp_slot(0, warp, NW, nsl, ushift);
+      if (VIS && sl >= 0) load_vis_words(p, g, valid, gslot0 + sl, n0, n1, n2);
+      for (int k = 1; sl >= 0; ++k) {
+        const int cur = sl;
+        sl = warp_slot(k, warp, NW, nsl, ushift);
         uint32_t w0 = n0, w1 = n1, w2 = n2;
         if (VIS) {
-          if (sl + 1 < sl1) load_vis_words(p, g, valid, gslot0 + sl + 1, n0, n1, n2);
+          if (sl >= 0) load_vis_words(p, g, valid, gslot0 + sl, n0, n1, n2);
           // skip a 32-point x 32-texel tile that is fully occluded for every lane
           if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
         }
-        const float4* rec = s_tab + 2 * (sl << 5);
+        const float4* rec = s_tab + 2 * (cur << 5);
 #pragma unroll 1
         for (int gq = 0; gq < 4; ++gq) {
 #pragma unroll
@@ -467,18 +487,21 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
         __syncthreads();
       }
       const int nsl = clen >> 5;
-      const int sl0 = (warp * nsl) / NW, sl1 = ((warp + 1) * nsl) / NW;
+      const int ushift = ((nsl + 1) >> 1) >= NW ? 1 : 0;
       const int gslot0 = cbase >> 5;
       const int ebase = p.env_in_smem ? 0 : cbase;
       uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
-      if (VIS && sl0 < sl1) load_vis_words(p, g, valid, gslot0 + sl0, n0, n1, n2);
-      for (int sl = sl0; sl < sl1; ++sl) {
+      int sl = warp_slot(0, warp, NW, nsl, ushift);
+      if (VIS && sl >= 0) load_vis_words(p, g, valid, gslot0 + sl, n0, n1, n2);
+      for (int k = 1; sl >= 0; ++k) {
+        const int cur = sl;
+        sl = warp_slot(k, warp, NW, nsl, ushift);
         uint32_t w0 = n0, w1 = n1, w2 = n2;
         if (VIS) {
-          if (sl + 1 < sl1) load_vis_words(p, g, valid, gslot0 + sl + 1, n0, n1, n2);
+          if (sl >= 0) load_vis_words(p, g, valid, gslot0 + sl, n0, n1, n2);
           if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
         }
-        const float4* rec = s_tab + 2 * (sl << 5);
+        const float4* rec = s_tab + 2 * (cur << 5);
 #pragma unroll 1
         for (int gq = 0; gq < 4; ++gq) {
           float wdj[8], wsj[8];
@@ -502,7 +525,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
           }
           if (!live) continue;
           // env-map gradient of these 8 texels: per lane e = gd * wd + gs * ws, summed over lanes
-          const int t0 = ebase + (sl << 5) + gq * 8;
+          const int t0 = ebase + (cur << 5) + gq * 8;
           const int jsel = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
           float e[8];
 #pragma unroll
