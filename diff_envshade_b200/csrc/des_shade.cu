@@ -303,7 +303,7 @@ __device__ __forceinline__ int warp_slot(int k, int warp, int NW, int nsl, int u
 // ------------------------------------------------------------------------------------------
 
 template <bool DIFF, bool SPEC, bool VIS>
-__global__ void __maxnreg__(80) des_fwd_kernel(const ShadeParams p) {
+__global__ void __maxnreg__(64) des_fwd_kernel(const ShadeParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* s_tab = reinterpret_cast<float4*>(smem_raw);
   float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)p.chunk * 32);
