@@ -195,6 +195,8 @@ __global__ void __launch_bounds__(kSortThreads, 1) des_prep_kernel(int H, int W,
       run += c;
     }
     counts[(size_t)k * ncp + blockIdx.x] = run;
+    if ((int)blockIdx.x == gridDim.x - 1)  // the padding columns of the row are zero
+      for (int q = gridDim.x; q < ncp; ++q) counts[(size_t)k * ncp + q] = 0u;
   }
   __syncthreads();
   if (nsub == 1) {
@@ -231,18 +233,19 @@ __global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chu
   const int k = threadIdx.x, lane = k & 31, w = k >> 5;
   const int c = blockIdx.x;
   const uint4* row = reinterpret_cast<const uint4*>(counts + (size_t)k * ncp);
+  // the row's padding columns (from nchunks to ncp) hold zeros
+  const int nq = ncp / 4, cq = c >> 2, cr = c & 3;
   unsigned pre = 0, tot = 0;
-  for (int q0 = 0; q0 < ncp / 4; q0 += 8) {
+  for (int q0 = 0; q0 < nq; q0 += 8) {
     uint4 v[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = (q0 + j < ncp / 4) ? row[q0 + j] : make_uint4(0u, 0u, 0u, 0u);
+    for (int j = 0; j < 8; ++j) v[j] = (q0 + j < nq) ? row[q0 + j] : make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const int c0 = 4 * (q0 + j);  // columns from nchunks on are padding (never written)
-      tot += (c0 < nchunks ? v[j].x : 0u) + (c0 + 1 < nchunks ? v[j].y : 0u) + (c0 + 2 < nchunks ? v[j].z : 0u) +
-             (c0 + 3 < nchunks ? v[j].w : 0u);
-      pre += (c0 < c ? v[j].x : 0u) + (c0 + 1 < c ? v[j].y : 0u) + (c0 + 2 < c ? v[j].z : 0u) +
-             (c0 + 3 < c ? v[j].w : 0u);
+      const unsigned sq = (v[j].x + v[j].y) + (v[j].z + v[j].w);
+      tot += sq;
+      if (q0 + j < cq) pre += sq;
+      if (q0 + j == cq) pre += (cr > 0 ? v[j].x : 0u) + (cr > 1 ? v[j].y : 0u) + (cr > 2 ? v[j].z : 0u);
     }
   }
   unsigned incl = tot;
