@@ -19,6 +19,11 @@ constexpr int kSortMinChunk = 1024;     // points ranked by one CTA: the smalles
 constexpr int kSortMaxChunks = 128;     //   multiple of 1024 that needs at most 128 CTAs
 constexpr int64_t kSortMinP = 16384;
 constexpr int64_t kSortMaxP = int64_t(1) << 24;  // per-warp 16-bit cell counters stay below 2^16
+inline int sort_chunk_for(int64_t P) {
+  int chunk = kSortMinChunk;
+  while ((int64_t)chunk * kSortMaxChunks < P) chunk *= 2;
+  return chunk;
+}
 
 // control words at the start of every workspace
 enum : int { kCtrlTileCounter = 0, kCtrlError = 1 };
@@ -93,6 +98,10 @@ int launch_texel_table(int H, int W, const float* R, float* out, des_stream_t st
 int launch_table(int H, int W, int HWpad, const float* R, const float* env, float4* rec, unsigned* ctrl,
                  cudaStream_t stream);
 void set_timing_events(cudaEvent_t start, cudaEvent_t stop);
+// Normal-direction ordering of P points on its own (kSortMinP..kSortMaxP points): perm[P] receives
+// the point indices in the order the shading kernels use; scratch needs point_order_scratch_bytes(P).
+size_t point_order_scratch_bytes(int64_t P);
+int launch_point_order(const float* normal, int64_t P, void* scratch, int32_t* perm, cudaStream_t stream);
 // Running count of kernel launches issued by this library (all streams and devices).
 void count_launches(int n);
 unsigned long long launches_so_far();

@@ -15,6 +15,24 @@ __device__ __forceinline__ void stage_table(float4* __restrict__ s_tab, const fl
   for (int i = threadIdx.x; i < 2 * len; i += blockDim.x) s_tab[i] = g_tab[2 * base + i];
 }
 
+// Point of tile slot `slot` (slot < P: the slot's lane is active).  With a permutation the point
+// is perm[slot]; an entry outside [0, P) sets error bit 8 and leaves the lane inactive instead of
+// being dereferenced.  Returns whether the lane is active; `pid` receives the point index.
+__device__ __forceinline__ bool ordered_point(const int32_t* __restrict__ perm, int64_t slot, int64_t P,
+                                              unsigned* ctrl, int64_t& pid) {
+  pid = slot;
+  if (slot >= P) return false;
+  if (perm == nullptr) return true;
+  const int32_t q = perm[slot];
+  if (q < 0 || (int64_t)q >= P) {
+    atomicOr(&ctrl[kCtrlError], 8u);
+    pid = 0;
+    return false;
+  }
+  pid = q;
+  return true;
+}
+
 struct PointGeom {
   float nx, ny, nz;  // normal (zeroed for inactive lanes: then no texel passes n.l > 0)
   float vx, vy, vz;  // view direction
@@ -143,6 +161,19 @@ __device__ __forceinline__ void pair_fwd_weights(const PointGeom& g, const SpecC
   }
 }
 
+
+// The k-th 32-texel slot (of nsl) integrated by warp `warp` of NW, or -1 past its last.  The
+// slots are taken in the order 0, nsl-1, 1, nsl-2, ... -- mirrored pairs, i.e. rows at opposite
+// elevations for the usual map widths -- and dealt to the warps a pair at a time (unit 2), or a
+// slot at a time when there are fewer pairs than warps (unit 1).  The horizon skip removes whole
+// rows for points that face up or down; mirrored pairs keep the surviving work of the warps of a
+// tile even, so they reach the end-of-tile barrier together.
+__device__ __forceinline__ int warp_slot(int k, int warp, int NW, int nsl, int ushift) {
+  // ushift = log2(unit)
+  const int j = (((k >> ushift) * NW + warp) << ushift) + (k & ushift);
+  if (j >= nsl) return -1;
+  return (j & 1) ? nsl - 1 - (j >> 1) : (j >> 1);
+}
 
 // Incoming gradients of one point folded with its albedos (bruteforce_shader.cu:2585-2588):
 // gd = g_shading * albedo + g_diffuse_shading, gs = g_shading * specular_albedo.

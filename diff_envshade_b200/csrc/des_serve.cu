@@ -3,16 +3,21 @@
 // Requests (forward, or forward + adjoint) of any point count arrive asynchronously.  A native
 // scheduler thread
 //   * admits them in arrival order while a device arena of fixed size (the HBM budget) has room,
-//     skipping over requests that do not fit yet, and uploads their point data on a copy stream;
+//     skipping over requests that do not fit yet, and uploads their point data through a copy lane
+//     that sends the least remaining work first, in slices (downloads use a second lane);
 //   * keeps env maps (their texel tables) and meshes (faces + visibility words) resident, shared by
 //     reference between requests;
 //   * every tick packs 32-point tiles of the admitted requests into a work list, smallest
-//     remaining work first, up to a time budget, and launches it as a CUDA graph (work-list upload
-//     + one persistent batch kernel) on one of two compute streams, so consecutive ticks overlap;
+//     remaining work first, up to a time budget, into a work list in mapped pinned memory and
+//     launches it as a CUDA graph (one persistent batch kernel) on its own stream, with up to
+//     ticks_in_flight ticks queued so that consecutive ticks overlap;
 //   * when every tile of a request has finished, copies its outputs back and frees its memory.
 // Work of different requests therefore shares each launch and each SM; a request that arrives
 // while others run joins the next tick.
 //
+// Requests of at least 16384 points are ordered by normal direction after their upload (the plain
+// path's ordering kernels, on a stream of their own), and the batch kernel skips texels below the
+// horizon of a warp's 32 points, as des_fwd_kernel / des_bwd_kernel do.
 // The batch kernel evaluates exactly the per-pair arithmetic of des_fwd_kernel / des_bwd_kernel
 // (shared helpers in des_point.cuh); per-point outputs are bit-identical to a solo call of the
 // batch path, and the env-map gradient is summed per request in FP64 (global FP64 atomics, then a
@@ -29,6 +34,9 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
+#include <unordered_set>
+#include <tuple>
 #include <thread>
 #include <vector>
 
@@ -45,6 +53,7 @@ constexpr int kMaxHWpad = 2048;      // texel table kept in shared memory per CT
 constexpr int kMaxSlots = 8192;      // concurrently admitted requests
 constexpr int kTickItems = 4096;     // work items per tick (upper bound; the whole list is uploaded)
 constexpr int kNTicks = 4;           // tick buffers (up to this many ticks in flight)
+constexpr int kCopyEvents = 64;                    // completion events per copy lane
 
 // Device-side request descriptor (member names shared with ShadeParams for the point loaders).
 struct ReqDesc {
@@ -73,6 +82,7 @@ struct ReqDesc {
   float* g_spec;
   float* g_rough;
   float* g_env;
+  const int32_t* perm;       // tile slot -> point (normal-direction order), or null for input order
   double* env_acc;           // [3][HWpad], zeroed at admission
   unsigned* bwd_tiles_left;  // adjoint tiles not yet finished
   unsigned* ctrl;            // [kCtrlError] = error word
@@ -89,27 +99,42 @@ struct SlotStage {
   unsigned pad[3];
 };
 
+// One tick's work, written by the scheduler into pinned host memory that the GPU reads directly
+// (mapped), so a tick needs no host-to-device copy: the batch kernel fetches each item over the
+// host link while it computes the previous one.
 struct WorkList {
-  unsigned counter, n, pad0, pad1;
+  unsigned n, pad0, pad1, pad2;
   WorkItem items[kTickItems];
+};
+
+// Device-side control of one tick buffer: [0] next item, [1] CTAs finished.  The last CTA of a
+// launch resets both, so every launch starts from zero without a host-side reset.
+struct TickCtl {
+  unsigned next, exited, pad0, pad1;
 };
 
 // ---------------------------------------------------------------------------------------------
 // Batch kernel
 // ---------------------------------------------------------------------------------------------
 
+// The tiles run the shading kernels' per-pair arithmetic with the same point ordering, horizon
+// skip and mirrored texel split (des_shade.cu), so per-point results equal the plain path's
+// arithmetic for the same point and texel, whatever else shares the launch.
 template <bool DIFF, bool SPEC, bool VIS>
 __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t pid = (int64_t)tile * 32 + lane;
-  const bool valid = pid < r.P;
+  const int64_t slot = (int64_t)tile * 32 + lane;
+  int64_t pid = slot;
+  const bool valid = ordered_point(r.perm, slot, r.P, r.ctrl, pid);
   const PointGeom g = load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
   SpecConst sc;
   if (SPEC) sc = spec_const(valid ? r.rough[pid] : 0.f, g);
   float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   const int nsl = r.HWpad >> 5;
-  const int sl0 = (warp * nsl) / kNW, sl1 = ((warp + 1) * nsl) / kNW;
-  for (int sl = sl0; sl < sl1; ++sl) {
+  const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
+  for (int k = 0;; ++k) {
+    const int sl = warp_slot(k, warp, kNW, nsl, ushift);
+    if (sl < 0) break;
     uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
     if (VIS) {
       load_vis_words(r, g, valid, sl, w0, w1, w2);
@@ -121,6 +146,7 @@ __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const float4 A = rec[2 * (gq * 8 + j)];
+        if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) continue;
         const float4 B = rec[2 * (gq * 8 + j) + 1];
         const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
         float wd, ws;
@@ -163,8 +189,9 @@ template <bool DIFF, bool SPEC, bool VIS>
 __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
   constexpr int NACC = 15;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t pid = (int64_t)tile * 32 + lane;
-  const bool valid = pid < r.P;
+  const int64_t slot = (int64_t)tile * 32 + lane;
+  int64_t pid = slot;
+  const bool valid = ordered_point(r.perm, slot, r.P, r.ctrl, pid);
   const PointGeom g = load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
   float gd0 = 0.f, gd1 = 0.f, gd2 = 0.f, gs0 = 0.f, gs1 = 0.f, gs2 = 0.f;
   if (valid) {
@@ -190,9 +217,11 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
   const BwdPoint gp{gd0, gd1, gd2, gs0, gs1, gs2};
   BwdAcc acc = {};
   const int nsl = r.HWpad >> 5;
-  const int sl0 = (warp * nsl) / kNW, sl1 = ((warp + 1) * nsl) / kNW;
+  const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
   const int jsel = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-  for (int sl = sl0; sl < sl1; ++sl) {
+  for (int k = 0;; ++k) {
+    const int sl = warp_slot(k, warp, kNW, nsl, ushift);
+    if (sl < 0) break;
     uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
     if (VIS) {
       load_vis_words(r, g, valid, sl, w0, w1, w2);
@@ -202,9 +231,14 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
 #pragma unroll 1
     for (int gq = 0; gq < 4; ++gq) {
       float wdj[8], wsj[8];
+      bool live = false;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
+        wdj[j] = 0.f;
+        wsj[j] = 0.f;
         const float4 A = rec[2 * (gq * 8 + j)];
+        if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) continue;
+        live = true;
         const float4 B = rec[2 * (gq * 8 + j) + 1];
         const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
         pair_bwd<DIFF, SPEC>(g, sc, gp, A, B, vis, acc, wdj[j], wsj[j]);
@@ -214,6 +248,7 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
         w1 >>= 8;
         w2 >>= 8;
       }
+      if (!live) continue;
       float e[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) e[j] = fmaf(gs0, wsj[j], gd0 * wdj[j]);
@@ -270,22 +305,33 @@ __device__ __forceinline__ void dispatch_tile(const ReqDesc& r, int tile, const 
   }
 }
 
-__global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __restrict__ reqs, WorkList* wl) {
+__global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __restrict__ reqs,
+                                                            const WorkList* __restrict__ wl, TickCtl* ctl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* s_tab = reinterpret_cast<float4*>(smem_raw);
   float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)kMaxHWpad * 32);
-  __shared__ int s_item[2];
+  __shared__ int s_idx[2];
+  __shared__ WorkItem s_item[2];
   __shared__ int s_last;
   const unsigned n = wl->n;
   int staged_req = -1;
   const float4* staged_table = nullptr;
-  if (threadIdx.x == 0) s_item[0] = (int)atomicAdd(&wl->counter, 1u);
+  // thread 0 fetches the index and the content of the next item one iteration ahead
+  if (threadIdx.x == 0) {
+    const int i0 = (int)atomicAdd(&ctl->next, 1u);
+    s_idx[0] = i0;
+    if (i0 < (int)n) s_item[0] = wl->items[i0];
+  }
   __syncthreads();
   for (int it = 0;; ++it) {
-    const int idx = s_item[it & 1];
+    const int idx = s_idx[it & 1];
     if (idx >= (int)n) break;
-    if (threadIdx.x == 0) s_item[(it + 1) & 1] = (int)atomicAdd(&wl->counter, 1u);
-    const WorkItem item = wl->items[idx];
+    const WorkItem item = s_item[it & 1];
+    if (threadIdx.x == 0) {
+      const int i1 = (int)atomicAdd(&ctl->next, 1u);
+      s_idx[(it + 1) & 1] = i1;
+      if (i1 < (int)n) s_item[(it + 1) & 1] = wl->items[i1];
+    }
     // a malformed work item is reported and skipped, never dereferenced
     if (item.req < 0 || item.req >= kMaxSlots || (item.kind != 0 && item.kind != 1) || item.tile < 0 ||
         (int64_t)item.tile * 32 >= reqs[item.req < 0 || item.req >= kMaxSlots ? 0 : item.req].P) {
@@ -320,6 +366,12 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
       }
     }
     __syncthreads();
+  }
+  // every CTA has made its last fetch before it counts itself out; the last one resets the tick
+  if (threadIdx.x == 0 && atomicAdd(&ctl->exited, 1u) == gridDim.x - 1) {
+    ctl->next = 0u;
+    ctl->exited = 0u;
+    __threadfence();
   }
 }
 
@@ -379,25 +431,138 @@ int64_t now_ns() {
       .count();
 }
 
-enum class State { Pending, Uploading, Ready, Downloading };
+enum class State { Pending, Uploading, Ordering, Ready, Downloading };
 
 struct Req {
   int64_t ticket;
   des_serve_request in;
   State state = State::Pending;
-  int64_t t_submit = 0, t_admit = 0;
+  int64_t t_submit = 0, t_admit = 0, t_uploaded = 0, t_ready = 0, t_computed = 0;
   size_t off = 0, bytes = 0;
   int slot = -1;
   int n_tiles = 0;
   int fwd_issued = 0, bwd_issued = 0, fwd_done = 0, bwd_done = 0;
   double cost_fwd_tile = 0, cost_bwd_tile = 0;
   ReqDesc desc{};
-  cudaEvent_t ev = nullptr;
+  int32_t* d_perm = nullptr;         // normal-direction order (P >= kSortMinP), else null
+  void* d_order_scratch = nullptr;
   // device pointers of outputs (for the download)
   float *d_shading = nullptr, *d_white = nullptr, *d_gn = nullptr, *d_gv = nullptr, *d_ga = nullptr,
         *d_gs = nullptr, *d_gr = nullptr, *d_genv = nullptr;
   double remaining() const {
     return (n_tiles - fwd_issued) * cost_fwd_tile + (in.backward ? (n_tiles - bwd_issued) * cost_bwd_tile : 0.0);
+  }
+};
+
+// Host<->device copies of the requests go through two copy lanes (one stream per direction, so
+// uploads and downloads overlap).  A request's copies form a job of segments; a lane issues its jobs
+// in slices, always from the job with the lowest priority value (least remaining work for uploads,
+// fewest bytes for downloads), and keeps a bounded number of bytes queued on its stream.  A small
+// request therefore waits for at most about one queue's worth of a large one's transfer instead
+// of all of it.  (Copies of one direction share a copy engine in submission order, so a short
+// queue is the only way to let a later, smaller request go first.)
+struct CopySeg {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+
+struct CopyJob {
+  Req* r = nullptr;
+  std::vector<CopySeg> segs;
+  size_t seg = 0, seg_off = 0;  // next byte to issue
+  int outstanding = 0;          // issued slices not yet complete
+  double prio = 0;              // lower goes first: the request's work (uploads), bytes (downloads)
+  bool issued_all() const { return seg >= segs.size(); }
+  void add(void* dst, const void* src, size_t bytes) {
+    if (bytes) segs.push_back(CopySeg{dst, src, bytes});
+  }
+};
+
+struct CopyLane {
+  struct Flight {
+    cudaEvent_t ev;
+    CopyJob* job;
+    size_t bytes;
+  };
+  cudaStream_t stream = nullptr;
+  cudaMemcpyKind kind = cudaMemcpyHostToDevice;
+  size_t slice = size_t(1) << 20;   // bytes per issued copy
+  size_t window = size_t(2) << 20;  // bytes queued on the stream at most
+  std::vector<CopyJob*> queue;  // jobs with slices left to issue, in arrival order
+  std::deque<Flight> flight;
+  std::vector<cudaEvent_t> free_ev;
+  size_t in_flight = 0;
+
+  bool init(cudaMemcpyKind k, size_t slice_bytes, size_t window_bytes) {
+    kind = k;
+    slice = slice_bytes;
+    window = window_bytes;
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return false;
+    for (int i = 0; i < kCopyEvents; ++i) {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+      free_ev.push_back(e);
+    }
+    return true;
+  }
+  void destroy() {
+    for (CopyJob* j : queue) delete j;
+    queue.clear();
+    for (auto& f : flight) {
+      free_ev.push_back(f.ev);
+      if (--f.job->outstanding == 0 && f.job->issued_all()) delete f.job;
+    }
+    flight.clear();
+    for (cudaEvent_t e : free_ev) cudaEventDestroy(e);
+    free_ev.clear();
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+  }
+  bool idle() const { return queue.empty() && flight.empty(); }
+  void pump();
+  // retires finished slices; appends jobs whose every slice has completed
+  // returns false when the stream reported an error (the server then fails its requests)
+  bool poll(std::vector<CopyJob*>& finished) {
+    while (!flight.empty()) {
+      const cudaError_t e = cudaEventQuery(flight.front().ev);
+      if (e == cudaErrorNotReady) break;
+      if (e != cudaSuccess) return false;
+      const Flight f = flight.front();
+      flight.pop_front();
+      free_ev.push_back(f.ev);
+      in_flight -= f.bytes;
+      if (--f.job->outstanding == 0 && f.job->issued_all()) finished.push_back(f.job);
+    }
+    return true;
+  }
+};
+
+// Normal-direction ordering of uploaded requests (the plain path's ordering kernels), on a stream
+// of its own so that it neither waits behind copies nor holds them up.
+struct OrderLane {
+  cudaStream_t stream = nullptr;
+  std::vector<cudaEvent_t> free_ev;
+  std::deque<std::pair<cudaEvent_t, Req*>> flight;
+  bool init() {
+    // highest priority: its few short CTAs take the first SMs that the persistent batch kernels free
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, greatest) != cudaSuccess) return false;
+    for (int i = 0; i < kCopyEvents; ++i) {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+      free_ev.push_back(e);
+    }
+    return true;
+  }
+  void destroy() {
+    for (auto& f : flight) free_ev.push_back(f.first);
+    flight.clear();
+    for (cudaEvent_t e : free_ev) cudaEventDestroy(e);
+    free_ev.clear();
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
   }
 };
 
@@ -412,10 +577,11 @@ struct Mesh {
 };
 
 struct Tick {
-  WorkList* h = nullptr;  // pinned
-  WorkList* d = nullptr;
+  double units = 0;       // work packed into the tick (pair units), for the throughput estimate
+  WorkList* h = nullptr;  // pinned, mapped
+  WorkList* d = nullptr;  // the device's address of h
+  TickCtl* ctl = nullptr;
   cudaGraphExec_t exec = nullptr;
-  cudaGraphNode_t copy_node = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   bool busy = false;
@@ -428,8 +594,11 @@ struct Tick {
 struct des_server {
   int device = 0;
   int tick_us = 150;
-  double pairs_per_us = 0;  // throughput estimate used to size ticks
-  cudaStream_t copy = nullptr;
+  double pairs_per_us = 0;   // throughput estimate used to size ticks (adapted to measured ticks)
+  double pairs_per_us0 = 0;  // starting estimate; the adapted value stays within 1/4x .. 4x of it
+  std::atomic<int> ticks_in_flight{3};  // tick buffers in use at once (<= kNTicks)
+  des::serve::CopyLane up, down;
+  des::serve::OrderLane order;
   unsigned char* arena_base = nullptr;
   des::serve::Arena arena;
   unsigned* d_ctrl = nullptr;
@@ -446,12 +615,16 @@ struct des_server {
   std::condition_variable cv;
   std::deque<des::serve::Req*> incoming;
   std::deque<des::serve::Req*> pending;
-  std::vector<des::serve::Req*> active;
+  std::unordered_set<des::serve::Req*> active;  // admitted, not yet reported done
+  // Ready requests with tiles left to issue, by (remaining work, ticket): the scheduling order
+  std::set<std::tuple<double, int64_t, des::serve::Req*>> ready;
+  int64_t last_tick_done_ns = 0;  // completion time of the previous tick (adaptive tick sizing)
   std::vector<des_serve_done> completed;
   int64_t next_ticket = 1;
   int64_t n_submitted = 0, n_done = 0;
   int error = DES_OK;
   std::atomic<bool> stop{false};
+  std::atomic<bool> failed{false};  // a CUDA error was seen: outstanding requests fail, submits are refused
   std::thread worker;
   int64_t t0 = 0;
   des_serve_stats stats{};
@@ -460,39 +633,93 @@ struct des_server {
 namespace des {
 namespace serve {
 
-namespace {
-
-size_t request_bytes(const des_serve_request& q, int HWpad, int HW) {
-  const size_t P = (size_t)q.P;
-  size_t b = 0;
-  auto add = [&](size_t n) { b += (n + 255) / 256 * 256; };
-  add(P * 12 * 4);  // normal, view, albedo, specular albedo
-  add(P * 4);       // roughness
-  if (q.mesh_id >= 0) {
-    add(P * 8);
-    add(P * 12);
+// Issues slices, job with the lowest priority value first, while the lane has room.
+void CopyLane::pump() {
+  while (in_flight < window && !queue.empty() && !free_ev.empty()) {
+    auto best = queue.begin();
+    for (auto it = queue.begin(); it != queue.end(); ++it)
+      if ((*it)->prio < (*best)->prio) best = it;
+    CopyJob* j = *best;
+    const CopySeg& sg = j->segs[j->seg];
+    const size_t n = std::min(slice, sg.bytes - j->seg_off);
+    cudaMemcpyAsync(static_cast<char*>(sg.dst) + j->seg_off, static_cast<const char*>(sg.src) + j->seg_off, n, kind,
+                    stream);
+    j->seg_off += n;
+    if (j->seg_off == sg.bytes) {
+      ++j->seg;
+      j->seg_off = 0;
+    }
+    cudaEvent_t ev = free_ev.back();
+    free_ev.pop_back();
+    cudaEventRecord(ev, stream);
+    flight.push_back(Flight{ev, j, n});
+    ++j->outstanding;
+    in_flight += n;
+    if (j->issued_all()) queue.erase(best);
   }
-  add(P * 12 * 2);  // shading, white
-  if (q.backward) {
-    add(P * 12 * 2);  // incoming gradients
-    add(P * 12 * 4 + P * 4);  // point gradients
-    add((size_t)3 * HWpad * 8);
-    add((size_t)3 * HW * 4);
-    add(256);
-  }
-  return b;
 }
 
-void upload(des_server* s, Req* r) {
-  const des_serve_request& q = r->in;
-  const Env& E = s->envs[q.env_id];
-  unsigned char* base = s->arena_base + r->off;
+namespace {
+
+// Device buffers of one request inside its arena range.  request_layout() both sizes the range
+// (base == nullptr) and hands out the pointers (base = the range's start), from one sequence of
+// 256-byte-aligned takes, so the two can never disagree.
+struct ReqLayout {
+  float *normal, *view, *albedo, *spec, *rough, *bary, *shading, *white, *gsh, *gwh, *grads, *genv;
+  int64_t* tri;
+  int32_t* perm;
+  void* order_scratch;
+  double* env_acc;
+  unsigned* tiles_left;
+  size_t bytes;
+};
+
+ReqLayout request_layout(const des_serve_request& q, const Env& E, unsigned char* base) {
+  ReqLayout L{};
   size_t off = 0;
-  auto take = [&](size_t n) {
-    unsigned char* p = base + off;
+  auto take = [&](size_t n) -> unsigned char* {
+    unsigned char* p = base ? base + off : nullptr;
     off += (n + 255) / 256 * 256;
     return p;
   };
+  const size_t P = (size_t)q.P;
+  L.normal = (float*)take(P * 12);
+  L.view = (float*)take(P * 12);
+  L.albedo = (float*)take(P * 12);
+  L.spec = (float*)take(P * 12);
+  L.rough = (float*)take(P * 4);
+  if (q.mesh_id >= 0) {
+    L.tri = (int64_t*)take(P * 8);
+    L.bary = (float*)take(P * 12);
+  }
+  L.shading = (float*)take(P * 12);
+  L.white = (float*)take(P * 12);
+  if (q.P >= kSortMinP && q.P <= kSortMaxP) {
+    L.perm = (int32_t*)take(P * 4);
+    L.order_scratch = take(point_order_scratch_bytes(q.P));
+  }
+  if (q.backward) {
+    L.gsh = (float*)take(P * 12);
+    L.gwh = (float*)take(P * 12);
+    L.grads = (float*)take(P * 12 * 4 + P * 4);
+    L.env_acc = (double*)take((size_t)3 * E.HWpad * 8);
+    L.genv = (float*)take((size_t)3 * E.H * E.W * 4);
+    L.tiles_left = (unsigned*)take(256);
+  }
+  L.bytes = off;
+  return L;
+}
+
+// Lays out the request's buffers in its arena range, fills its device descriptor and queues its
+// uploads on the upload lane (descriptor, counters and the env-gradient accumulator are set up
+// right away; the point data goes in prioritised slices).
+void upload(des_server* s, Req* r) {
+  const des_serve_request& q = r->in;
+  const Env& E = s->envs[q.env_id];
+  const ReqLayout L = request_layout(q, E, s->arena_base + r->off);
+  CopyLane& lane = s->up;
+  auto* job = new CopyJob();
+  job->r = r;
   const size_t P = (size_t)q.P;
   ReqDesc& d = r->desc;
   d = ReqDesc{};
@@ -504,48 +731,43 @@ void upload(des_server* s, Req* r) {
   d.clamp = (q.flags & DES_CLAMP) != 0;
   d.table = E.table;
   d.ctrl = s->d_ctrl;
-  float* normal = (float*)take(P * 12);
-  float* view = (float*)take(P * 12);
-  float* albedo = (float*)take(P * 12);
-  float* spec = (float*)take(P * 12);
-  float* rough = (float*)take(P * 4);
-  cudaMemcpyAsync(normal, q.normal, P * 12, cudaMemcpyHostToDevice, s->copy);
-  cudaMemcpyAsync(view, q.view_dir, P * 12, cudaMemcpyHostToDevice, s->copy);
-  cudaMemcpyAsync(albedo, q.albedo, P * 12, cudaMemcpyHostToDevice, s->copy);
-  cudaMemcpyAsync(spec, q.specular_albedo, P * 12, cudaMemcpyHostToDevice, s->copy);
-  cudaMemcpyAsync(rough, q.roughness, P * 4, cudaMemcpyHostToDevice, s->copy);
-  d.normal = normal;
-  d.view = view;
-  d.albedo = albedo;
-  d.spec_alb = spec;
-  d.rough = rough;
+  job->add(L.normal, q.normal, P * 12);
+  job->add(L.view, q.view_dir, P * 12);
+  job->add(L.albedo, q.albedo, P * 12);
+  job->add(L.spec, q.specular_albedo, P * 12);
+  job->add(L.rough, q.roughness, P * 4);
+  d.normal = L.normal;
+  d.view = L.view;
+  d.albedo = L.albedo;
+  d.spec_alb = L.spec;
+  d.rough = L.rough;
   if (q.mesh_id >= 0) {
     const Mesh& M = s->meshes[q.mesh_id];
-    int64_t* tri = (int64_t*)take(P * 8);
-    float* bary = (float*)take(P * 12);
-    cudaMemcpyAsync(tri, q.nearest_triangle_id, P * 8, cudaMemcpyHostToDevice, s->copy);
-    cudaMemcpyAsync(bary, q.barycentric_coord, P * 12, cudaMemcpyHostToDevice, s->copy);
+    job->add(L.tri, q.nearest_triangle_id, P * 8);
+    job->add(L.bary, q.barycentric_coord, P * 12);
     d.has_vis = 1;
     d.N_face = M.N_face;
     d.N_vertex = M.N_vertex;
     d.faces = M.faces;
     d.vis = M.vis;
-    d.tri = tri;
-    d.bary = bary;
+    d.tri = L.tri;
+    d.bary = L.bary;
   }
-  r->d_shading = (float*)take(P * 12);
-  r->d_white = (float*)take(P * 12);
-  d.shading = r->d_shading;
-  d.white = r->d_white;
+  r->d_shading = L.shading;
+  r->d_white = L.white;
+  d.shading = L.shading;
+  d.white = L.white;
+  if (L.perm != nullptr) {
+    r->d_perm = L.perm;
+    r->d_order_scratch = L.order_scratch;
+    d.perm = L.perm;  // read only once the request is Ready, i.e. after its ordering
+  }
   if (q.backward) {
-    float* gsh = (float*)take(P * 12);
-    float* gwh = (float*)take(P * 12);
-    cudaMemcpyAsync(gsh, q.grad_shading, P * 12, cudaMemcpyHostToDevice, s->copy);
-    if (q.grad_diffuse_shading) cudaMemcpyAsync(gwh, q.grad_diffuse_shading, P * 12, cudaMemcpyHostToDevice, s->copy);
-    d.g_shading = gsh;
-    d.g_white = q.grad_diffuse_shading ? gwh : nullptr;
-    unsigned char* g = take(P * 12 * 4 + P * 4);
-    r->d_gn = (float*)g;
+    job->add(L.gsh, q.grad_shading, P * 12);
+    if (q.grad_diffuse_shading) job->add(L.gwh, q.grad_diffuse_shading, P * 12);
+    d.g_shading = L.gsh;
+    d.g_white = q.grad_diffuse_shading ? L.gwh : nullptr;
+    r->d_gn = L.grads;
     r->d_gv = r->d_gn + 3 * P;
     r->d_ga = r->d_gv + 3 * P;
     r->d_gs = r->d_ga + 3 * P;
@@ -555,59 +777,63 @@ void upload(des_server* s, Req* r) {
     d.g_albedo = r->d_ga;
     d.g_spec = r->d_gs;
     d.g_rough = r->d_gr;
-    d.env_acc = (double*)take((size_t)3 * E.HWpad * 8);
-    r->d_genv = (float*)take((size_t)3 * d.HW * 4);
-    d.g_env = r->d_genv;
-    d.bwd_tiles_left = (unsigned*)take(256);
-    cudaMemsetAsync(d.env_acc, 0, (size_t)3 * E.HWpad * 8, s->copy);
+    d.env_acc = L.env_acc;
+    r->d_genv = L.genv;
+    d.g_env = L.genv;
+    d.bwd_tiles_left = L.tiles_left;
+    cudaMemsetAsync(d.env_acc, 0, (size_t)3 * E.HWpad * 8, lane.stream);
     s->h_stage[r->slot].tiles_left = (unsigned)r->n_tiles;
     cudaMemcpyAsync(d.bwd_tiles_left, &s->h_stage[r->slot].tiles_left, sizeof(unsigned), cudaMemcpyHostToDevice,
-                    s->copy);
+                    lane.stream);
   }
   s->h_stage[r->slot].desc = d;
-  cudaMemcpyAsync(&s->d_reqs[r->slot], &s->h_stage[r->slot].desc, sizeof(ReqDesc), cudaMemcpyHostToDevice, s->copy);
-  cudaEventRecord(r->ev, s->copy);
+  cudaMemcpyAsync(&s->d_reqs[r->slot], &s->h_stage[r->slot].desc, sizeof(ReqDesc), cudaMemcpyHostToDevice,
+                  lane.stream);
+  job->prio = r->remaining();
+  lane.queue.push_back(job);
 }
 
+// Queues the request's outputs on the download lane.
 void download(des_server* s, Req* r) {
   const des_serve_request& q = r->in;
   const size_t P = (size_t)q.P;
   const Env& E = s->envs[q.env_id];
-  if (q.shading) cudaMemcpyAsync(q.shading, r->d_shading, P * 12, cudaMemcpyDeviceToHost, s->copy);
-  if (q.diffuse_shading) cudaMemcpyAsync(q.diffuse_shading, r->d_white, P * 12, cudaMemcpyDeviceToHost, s->copy);
+  auto* job = new CopyJob();
+  job->r = r;
+  if (q.shading) job->add(q.shading, r->d_shading, P * 12);
+  if (q.diffuse_shading) job->add(q.diffuse_shading, r->d_white, P * 12);
   if (q.backward) {
-    if (q.g_normal) cudaMemcpyAsync(q.g_normal, r->d_gn, P * 12, cudaMemcpyDeviceToHost, s->copy);
-    if (q.g_view_dir) cudaMemcpyAsync(q.g_view_dir, r->d_gv, P * 12, cudaMemcpyDeviceToHost, s->copy);
-    if (q.g_albedo) cudaMemcpyAsync(q.g_albedo, r->d_ga, P * 12, cudaMemcpyDeviceToHost, s->copy);
-    if (q.g_specular_albedo) cudaMemcpyAsync(q.g_specular_albedo, r->d_gs, P * 12, cudaMemcpyDeviceToHost, s->copy);
-    if (q.g_roughness) cudaMemcpyAsync(q.g_roughness, r->d_gr, P * 4, cudaMemcpyDeviceToHost, s->copy);
-    if (q.g_envmap)
-      cudaMemcpyAsync(q.g_envmap, r->d_genv, (size_t)3 * E.H * E.W * 4, cudaMemcpyDeviceToHost, s->copy);
+    if (q.g_normal) job->add(q.g_normal, r->d_gn, P * 12);
+    if (q.g_view_dir) job->add(q.g_view_dir, r->d_gv, P * 12);
+    if (q.g_albedo) job->add(q.g_albedo, r->d_ga, P * 12);
+    if (q.g_specular_albedo) job->add(q.g_specular_albedo, r->d_gs, P * 12);
+    if (q.g_roughness) job->add(q.g_roughness, r->d_gr, P * 4);
+    if (q.g_envmap) job->add(q.g_envmap, r->d_genv, (size_t)3 * E.H * E.W * 4);
   }
-  cudaEventRecord(r->ev, s->copy);
+  for (const CopySeg& sg : job->segs) job->prio += (double)sg.bytes;
+  s->down.queue.push_back(job);
 }
 
 // Builds and launches one tick if a tick buffer is free.  Returns true when work was launched.
 bool launch_tick(des_server* s) {
   Tick* t = nullptr;
-  for (auto& k : s->ticks)
-    if (!k.busy) {
+  int busy = 0;
+  for (auto& k : s->ticks) {
+    if (k.busy)
+      ++busy;
+    else if (t == nullptr)
       t = &k;
-      break;
-    }
-  if (t == nullptr) return false;
-  std::vector<Req*> ready;
-  for (Req* r : s->active)
-    if (r->state == State::Ready && r->remaining() > 0) ready.push_back(r);
-  if (ready.empty()) return false;
-  // shortest remaining work first; ties by arrival
-  std::stable_sort(ready.begin(), ready.end(), [](const Req* a, const Req* b) { return a->remaining() < b->remaining(); });
+  }
+  if (t == nullptr || busy >= s->ticks_in_flight) return false;
+  if (s->ready.empty()) return false;
+  // shortest remaining work first, ties by arrival (the set's order)
   const double budget = s->pairs_per_us * s->tick_us;
   double used = 0;
   unsigned n = 0;
   t->counts.clear();
-  for (Req* r : ready) {
-    if (used >= budget || n >= (unsigned)kTickItems) break;
+  while (!s->ready.empty() && used < budget && n < (unsigned)kTickItems) {
+    Req* r = std::get<2>(*s->ready.begin());
+    s->ready.erase(s->ready.begin());
     int nf = 0, nb = 0;
     while (used < budget && n < (unsigned)kTickItems && (r->fwd_issued < r->n_tiles ||
                                                           (r->in.backward && r->bwd_issued < r->n_tiles))) {
@@ -623,15 +849,16 @@ bool launch_tick(des_server* s) {
       }
     }
     t->counts.push_back({r, {nf, nb}});
+    if (r->remaining() > 0) s->ready.insert({r->remaining(), r->ticket, r});  // budget is used up
   }
-  t->h->counter = 0;
+  t->units = used;
   t->h->n = n;
+  std::atomic_thread_fence(std::memory_order_seq_cst);  // items are in host memory before the launch
   if (cudaGraphLaunch(t->exec, t->stream) != cudaSuccess) {
     // launch the same work without the graph
     cudaGetLastError();
-    cudaMemcpyAsync(t->d, t->h, sizeof(WorkList), cudaMemcpyHostToDevice, t->stream);
-    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_reqs, t->d);
-    s->stats.device_error |= 8;
+    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_reqs, t->d, t->ctl);
+    s->stats.device_error |= 16;
   }
   count_launches(1);
   cudaEventRecord(t->done, t->stream);
@@ -653,11 +880,37 @@ void worker_loop(des_server* s) {
         s->incoming.pop_front();
       }
     }
+    // 0. after a CUDA error nothing more can complete: fail every outstanding request at once
+    if (s->failed) {
+      std::vector<Req*> all(s->active.begin(), s->active.end());
+      all.insert(all.end(), s->pending.begin(), s->pending.end());
+      s->active.clear();
+      s->pending.clear();
+      s->ready.clear();
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (Req* r : all) {
+          des_serve_done d{};
+          d.ticket = r->ticket;
+          d.t_submit_ns = r->t_submit - s->t0;
+          d.t_done_ns = now_ns() - s->t0;
+          d.status = DES_ERR_CUDA;
+          s->completed.push_back(d);
+          s->n_done += 1;
+          delete r;
+        }
+        s->error = DES_ERR_CUDA;
+      }
+      s->cv.notify_all();
+      if (s->stop) break;
+      std::this_thread::sleep_for(std::chrono::microseconds(200));
+      continue;
+    }
     // 1. admission (arrival order; requests that do not fit yet are skipped, not blocking others)
     for (auto it = s->pending.begin(); it != s->pending.end();) {
       Req* r = *it;
       const Env& E = s->envs[r->in.env_id];
-      r->bytes = request_bytes(r->in, E.HWpad, E.H * E.W);
+      r->bytes = request_layout(r->in, E, nullptr).bytes;
       size_t off = 0;
       if (s->free_slots.empty() || !s->arena.alloc(r->bytes, &off)) {
         ++it;
@@ -673,61 +926,128 @@ void worker_loop(des_server* s) {
       r->cost_bwd_tile = 2.0 * pairs;
       upload(s, r);
       r->state = State::Uploading;
-      s->active.push_back(r);
+      s->active.insert(r);
       it = s->pending.erase(it);
       progressed = true;
       s->stats.peak_arena_bytes = std::max<int64_t>(s->stats.peak_arena_bytes, (int64_t)s->arena.used());
     }
     // 2. finished ticks
     for (auto& t : s->ticks) {
-      if (t.busy && cudaEventQuery(t.done) == cudaSuccess) {
+      if (!t.busy) continue;
+      const cudaError_t te = cudaEventQuery(t.done);
+      if (te != cudaSuccess && te != cudaErrorNotReady) s->failed = true;
+      if (te == cudaSuccess) {
+        // throughput estimate: work of this tick over the time since the previous completion,
+        // taken only while the GPU had a further tick queued (no idle gap in between)
+        const int64_t tnow = now_ns();
+        int others = 0;
+        for (auto& o : s->ticks) others += (o.busy && &o != &t) ? 1 : 0;
+        if (s->last_tick_done_ns > 0 && others > 0 && t.units > 0) {
+          const double us = (tnow - s->last_tick_done_ns) * 1e-3;
+          if (us > 5.0) {
+            const double rate = std::min(std::max(t.units / us, 0.25 * s->pairs_per_us0), 4.0 * s->pairs_per_us0);
+            s->pairs_per_us = 0.9 * s->pairs_per_us + 0.1 * rate;
+          }
+        }
+        s->last_tick_done_ns = tnow;
         for (auto& c : t.counts) {
-          c.first->fwd_done += c.second.first;
-          c.first->bwd_done += c.second.second;
+          Req* r = c.first;
+          r->fwd_done += c.second.first;
+          r->bwd_done += c.second.second;
+          if (r->state == State::Ready && r->fwd_done == r->n_tiles && (!r->in.backward || r->bwd_done == r->n_tiles)) {
+            r->t_computed = tnow;
+            download(s, r);
+            r->state = State::Downloading;
+          }
         }
         t.counts.clear();
         t.busy = false;
         progressed = true;
       }
     }
-    // 3. request state transitions
-    for (auto it = s->active.begin(); it != s->active.end();) {
-      Req* r = *it;
-      if (r->state == State::Uploading && cudaEventQuery(r->ev) == cudaSuccess) {
-        r->state = State::Ready;
-        progressed = true;
-      }
-      if (r->state == State::Ready && r->fwd_done == r->n_tiles && (!r->in.backward || r->bwd_done == r->n_tiles)) {
-        download(s, r);
-        r->state = State::Downloading;
-        progressed = true;
-      }
-      if (r->state == State::Downloading && cudaEventQuery(r->ev) == cudaSuccess) {
-        des_serve_done d{};
-        d.ticket = r->ticket;
-        d.t_submit_ns = r->t_submit - s->t0;
-        d.t_admit_ns = r->t_admit - s->t0;
-        d.t_done_ns = now_ns() - s->t0;
-        d.status = DES_OK;
-        s->arena.release(r->off, r->bytes);
-        s->free_slots.push_back(r->slot);
-        cudaEventDestroy(r->ev);
-        {
-          std::lock_guard<std::mutex> lk(s->mu);
-          s->completed.push_back(d);
-          s->n_done += 1;
+    // 3. copies: retire finished slices, then issue more
+    std::vector<CopyJob*> fin;
+    if (!s->up.poll(fin)) s->failed = true;
+    for (CopyJob* j : fin) {
+      Req* r = j->r;
+      delete j;
+      progressed = true;
+      r->t_uploaded = now_ns();
+      if (r->d_perm != nullptr && !s->order.free_ev.empty() &&
+          launch_point_order(r->desc.normal, r->in.P, r->d_order_scratch, r->d_perm, s->order.stream) == DES_OK) {
+        cudaEvent_t ev = s->order.free_ev.back();
+        s->order.free_ev.pop_back();
+        cudaEventRecord(ev, s->order.stream);
+        s->order.flight.push_back({ev, r});
+        r->state = State::Ordering;
+      } else {
+        if (r->d_perm != nullptr) {  // no ordering after all: shade in input order
+          r->desc.perm = nullptr;
+          s->h_stage[r->slot].desc.perm = nullptr;
+          cudaMemcpyAsync(&s->d_reqs[r->slot].perm, &s->h_stage[r->slot].desc.perm, sizeof(void*),
+                          cudaMemcpyHostToDevice, s->order.stream);
+          cudaStreamSynchronize(s->order.stream);
         }
-        s->cv.notify_all();
-        delete r;
-        it = s->active.erase(it);
-        progressed = true;
-        continue;
+        r->state = State::Ready;
+        r->t_ready = now_ns();
+        s->ready.insert({r->remaining(), r->ticket, r});
       }
-      ++it;
     }
-    // 4. new ticks
+    while (!s->order.flight.empty()) {
+      const cudaError_t oe = cudaEventQuery(s->order.flight.front().first);
+      if (oe == cudaErrorNotReady) break;
+      if (oe != cudaSuccess) {
+        s->failed = true;
+        break;
+      }
+      Req* r = s->order.flight.front().second;
+      s->order.free_ev.push_back(s->order.flight.front().first);
+      s->order.flight.pop_front();
+      r->state = State::Ready;
+      r->t_ready = now_ns();
+      s->ready.insert({r->remaining(), r->ticket, r});
+      progressed = true;
+    }
+    fin.clear();
+    if (!s->down.poll(fin)) s->failed = true;
+    for (CopyJob* j : fin) {
+      Req* r = j->r;
+      delete j;
+      progressed = true;
+      des_serve_done d{};
+      d.ticket = r->ticket;
+      d.t_submit_ns = r->t_submit - s->t0;
+      d.t_admit_ns = r->t_admit - s->t0;
+      d.t_uploaded_ns = r->t_uploaded - s->t0;
+      d.t_ready_ns = r->t_ready - s->t0;
+      d.t_computed_ns = r->t_computed - s->t0;
+      d.t_done_ns = now_ns() - s->t0;
+      d.status = DES_OK;
+      s->arena.release(r->off, r->bytes);
+      s->free_slots.push_back(r->slot);
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->completed.push_back(d);
+        s->n_done += 1;
+      }
+      s->cv.notify_all();
+      s->active.erase(r);
+      delete r;
+    }
+    // 4. new ticks, new copies
     while (launch_tick(s)) progressed = true;
-    if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(10));
+    s->up.pump();
+    s->down.pump();
+    if (!progressed) {
+      // poll without sleeping while the GPU or a copy lane has work (a sleep costs ~50 us of
+      // reaction time); sleep only when everything is idle
+      bool busy = !s->up.idle() || !s->down.idle() || !s->order.flight.empty();
+      for (auto& t : s->ticks) busy = busy || t.busy;
+      if (busy)
+        std::this_thread::yield();
+      else
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
   }
 }
 
@@ -755,7 +1075,9 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
   // a conservative starting throughput; it only sizes ticks
   s->pairs_per_us = 1.5e5 * s->sms / 148.0;
-  bool ok = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking) == cudaSuccess &&
+  s->pairs_per_us0 = s->pairs_per_us;
+  bool ok = s->up.init(cudaMemcpyHostToDevice, size_t(1) << 20, size_t(4) << 20) &&
+            s->down.init(cudaMemcpyDeviceToHost, size_t(1) << 20, size_t(4) << 20) && s->order.init() &&
             cudaMalloc(&s->arena_base, hbm_budget_bytes) == cudaSuccess &&
             cudaMalloc(&s->d_ctrl, 256) == cudaSuccess &&
             cudaMalloc(&s->d_reqs, sizeof(des::serve::ReqDesc) * des::serve::kMaxSlots) == cudaSuccess &&
@@ -776,33 +1098,25 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, des::serve::batch_kernel, des::serve::kNW * 32, s->smem);
   s->grid = std::max(1, occ) * s->sms;
-  // one captured graph per tick buffer: work-list upload + the persistent batch kernel
+  // one captured graph per tick buffer: the persistent batch kernel over that buffer's work list
   for (auto& t : s->ticks) {
-    ok = cudaMallocHost(&t.h, sizeof(des::serve::WorkList)) == cudaSuccess &&
-         cudaMalloc(&t.d, sizeof(des::serve::WorkList)) == cudaSuccess &&
+    ok = cudaHostAlloc(&t.h, sizeof(des::serve::WorkList), cudaHostAllocMapped) == cudaSuccess &&
+         cudaHostGetDevicePointer(reinterpret_cast<void**>(&t.d), t.h, 0) == cudaSuccess &&
+         cudaMalloc(&t.ctl, sizeof(des::serve::TickCtl)) == cudaSuccess &&
+         cudaMemset(t.ctl, 0, sizeof(des::serve::TickCtl)) == cudaSuccess &&
          cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking) == cudaSuccess &&
-         cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming) == cudaSuccess;
+         cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming) == cudaSuccess &&
+         cudaDeviceSynchronize() == cudaSuccess;
     if (!ok) {
       des_server_destroy(s);
       return DES_ERR_CUDA;
     }
     std::memset(t.h, 0, sizeof(des::serve::WorkList));
-    cudaMemset(t.d, 0, sizeof(des::serve::WorkList));
     cudaGraph_t g = nullptr;
     ok = cudaStreamBeginCapture(t.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    cudaMemcpyAsync(t.d, t.h, sizeof(des::serve::WorkList), cudaMemcpyHostToDevice, t.stream);
-    des::serve::batch_kernel<<<s->grid, des::serve::kNW * 32, s->smem, t.stream>>>(s->d_reqs, t.d);
+    des::serve::batch_kernel<<<s->grid, des::serve::kNW * 32, s->smem, t.stream>>>(s->d_reqs, t.d, t.ctl);
     ok = ok && cudaStreamEndCapture(t.stream, &g) == cudaSuccess;
-    size_t nn = 0;
-    ok = ok && cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn == 2;
-    cudaGraphNode_t nodes[2];
-    ok = ok && cudaGraphGetNodes(g, nodes, &nn) == cudaSuccess;
-    if (ok) {
-      cudaGraphNodeType ty;
-      cudaGraphNodeGetType(nodes[0], &ty);
-      t.copy_node = (ty == cudaGraphNodeTypeMemcpy) ? nodes[0] : nodes[1];
-      ok = cudaGraphInstantiate(&t.exec, g, 0) == cudaSuccess;
-    }
+    ok = ok && cudaGraphInstantiate(&t.exec, g, 0) == cudaSuccess;
     if (g) cudaGraphDestroy(g);
     if (!ok) {
       des_server_destroy(s);
@@ -879,14 +1193,11 @@ int des_server_submit(des_server* s, const des_serve_request* req, int64_t* tick
   if (req->backward && !req->grad_shading) return DES_ERR_INVALID_ARGUMENT;
   if (!(req->flags & (DES_DIFFUSE | DES_SPECULAR)) || (req->flags & ~(unsigned)(DES_DIFFUSE | DES_SPECULAR | DES_CLAMP)))
     return DES_ERR_INVALID_ARGUMENT;
+  if (s->failed) return DES_ERR_CUDA;
   auto* r = new Req();
   r->ticket = s->next_ticket++;
   r->in = *req;
   r->t_submit = des::serve::now_ns();
-  if (cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess) {
-    delete r;
-    return DES_ERR_CUDA;
-  }
   s->incoming.push_back(r);
   s->n_submitted += 1;
   *ticket = r->ticket;
@@ -909,6 +1220,13 @@ int des_server_drain(des_server* s, int timeout_ms) {
   const bool done = s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms),
                                    [&] { return s->n_done == s->n_submitted; });
   return done ? DES_OK : DES_ERR_TIMEOUT;
+}
+
+int des_server_set_ticks_in_flight(des_server* s, int n) {
+  if (s == nullptr || n < 1 || n > des::serve::kNTicks) return DES_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->ticks_in_flight = n;
+  return DES_OK;
 }
 
 int des_server_stats(des_server* s, des_serve_stats* out) {
@@ -934,7 +1252,7 @@ int des_server_destroy(des_server* s) {
   for (auto& t : s->ticks) {
     if (t.exec) cudaGraphExecDestroy(t.exec);
     if (t.h) cudaFreeHost(t.h);
-    if (t.d) cudaFree(t.d);
+    if (t.ctl) cudaFree(t.ctl);
     if (t.done) cudaEventDestroy(t.done);
     if (t.stream) cudaStreamDestroy(t.stream);
   }
@@ -949,7 +1267,9 @@ int des_server_destroy(des_server* s) {
   if (s->d_reqs) cudaFree(s->d_reqs);
   if (s->d_ctrl) cudaFree(s->d_ctrl);
   if (s->arena_base) cudaFree(s->arena_base);
-  if (s->copy) cudaStreamDestroy(s->copy);
+  s->up.destroy();
+  s->down.destroy();
+  s->order.destroy();
   delete s;
   return DES_OK;
 }

@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kSortThreads, 1) des_prep_kernel(int H, int W,
   constexpr int SUB = 2 * kSortThreads;  // points per pass: 2 rounds per warp
   __shared__ uint16_t cnt[NW][kSortBins];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  if (blockIdx.x == 0 && tid == 0) {
+  if (blockIdx.x == 0 && tid == 0 && ctrl != nullptr) {
     ctrl[kCtrlTileCounter] = 0u;
     ctrl[kCtrlError] = 0u;
   }
@@ -286,22 +286,6 @@ __global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chu
 }
 
 // ------------------------------------------------------------------------------------------
-// Texel split between the warps of a tile
-// ------------------------------------------------------------------------------------------
-// The k-th 32-texel slot (of nsl) integrated by warp `warp` of NW, or -1 past its last.  The
-// slots are taken in the order 0, nsl-1, 1, nsl-2, ... -- mirrored pairs, i.e. rows at opposite
-// elevations for the usual map widths -- and dealt to the warps a pair at a time (unit 2), or a
-// slot at a time when there are fewer pairs than warps (unit 1).  The horizon skip removes whole
-// rows for points that face up or down; mirrored pairs keep the surviving work of the warps of a
-// tile even, so they reach the end-of-tile barrier together.
-__device__ __forceinline__ int warp_slot(int k, int warp, int NW, int nsl, int ushift) {
-  // ushift = log2(unit)
-  const int j = (((k >> ushift) * NW + warp) << ushift) + (k & ushift);
-  if (j >= nsl) return -1;
-  return (j & 1) ? nsl - 1 - (j >> 1) : (j >> 1);
-}
-
-// ------------------------------------------------------------------------------------------
 // Forward
 // ------------------------------------------------------------------------------------------
 
@@ -328,8 +312,8 @@ __global__ void __maxnreg__(64) des_fwd_kernel(const ShadeParams p) {
     if (threadIdx.x == 0) s_next[it & 1] = (int)gridDim.x + (int)atomicAdd(&p.ctrl[kCtrlTileCounter], 1u);
 
     const int64_t slot = (int64_t)tile * 32 + lane;
-    const bool valid = slot < p.P;
-    const int64_t pid = (valid && p.perm != nullptr) ? (int64_t)p.perm[slot] : slot;
+    int64_t pid = slot;
+    const bool valid = ordered_point(p.perm, slot, p.P, p.ctrl, pid);
     const PointGeom g = load_geom<VIS>(p, pid, valid, need_view);
     SpecConst sc;
     if (SPEC) sc = spec_const(valid ? p.rough[pid] : 0.f, g);
@@ -452,8 +436,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
     if (threadIdx.x == 0) s_next[it & 1] = (int)gridDim.x + (int)atomicAdd(&p.ctrl[kCtrlTileCounter], 1u);
 
     const int64_t slot = (int64_t)tile * 32 + lane;
-    const bool valid = slot < p.P;
-    const int64_t pid = (valid && p.perm != nullptr) ? (int64_t)p.perm[slot] : slot;
+    int64_t pid = slot;
+    const bool valid = ordered_point(p.perm, slot, p.P, p.ctrl, pid);
     const PointGeom g = load_geom<VIS>(p, pid, valid, need_view);
     // incoming gradients folded with the albedos (bruteforce_shader.cu:2585-2588)
     float gd0 = 0.f, gd1 = 0.f, gd2 = 0.f, gs0 = 0.f, gs1 = 0.f, gs2 = 0.f;
@@ -705,8 +689,7 @@ LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev) {
   lp.sms = di.sms;
   lp.max_smem = di.max_smem_optin;
   lp.sort = P >= kSortMinP && P <= kSortMaxP;
-  lp.sort_chunk = kSortMinChunk;
-  while ((int64_t)lp.sort_chunk * kSortMaxChunks < P) lp.sort_chunk *= 2;
+  lp.sort_chunk = sort_chunk_for(P);
   lp.sort_chunks = lp.sort ? (int)((P + lp.sort_chunk - 1) / lp.sort_chunk) : 0;
   return lp;
 }
@@ -886,6 +869,28 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
     count_launches(1);
   }
   return DES_OK;
+}
+
+size_t point_order_scratch_bytes(int64_t P) {
+  const int64_t chunk = sort_chunk_for(P), nchunks = (P + chunk - 1) / chunk, ncp = (nchunks + 3) / 4 * 4;
+  return align_up((size_t)kSortBins * ncp * sizeof(unsigned), 256) + align_up((size_t)P * sizeof(uint16_t), 256) +
+         align_up((size_t)P * sizeof(uint32_t), 256);
+}
+
+int launch_point_order(const float* normal, int64_t P, void* scratch, int32_t* perm, cudaStream_t stream) {
+  if (P <= 0 || P > kSortMaxP) return DES_ERR_INVALID_ARGUMENT;
+  const int chunk = sort_chunk_for(P);
+  const int nchunks = (int)((P + chunk - 1) / chunk), ncp = (nchunks + 3) / 4 * 4;
+  unsigned* counts = static_cast<unsigned*>(scratch);
+  uint16_t* keys = reinterpret_cast<uint16_t*>(static_cast<unsigned char*>(scratch) +
+                                               align_up((size_t)kSortBins * ncp * sizeof(unsigned), 256));
+  uint32_t* rank = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(keys) +
+                                               align_up((size_t)P * sizeof(uint16_t), 256));
+  des_prep_kernel<<<nchunks, kSortThreads, 0, stream>>>(0, 0, 0, nullptr, nullptr, nullptr, nullptr, normal, P, chunk,
+                                                        ncp, counts, keys, rank);
+  des_place_kernel<<<nchunks, kSortBins, 0, stream>>>(P, chunk, nchunks, ncp, counts, keys, rank, perm);
+  count_launches(2);
+  return cudaGetLastError() == cudaSuccess ? DES_OK : DES_ERR_CUDA;
 }
 
 int launch_table(int H, int W, int HWpad, const float* R, const float* env, float4* rec, unsigned* ctrl,

@@ -97,9 +97,10 @@ def _summarize(lat_s, sched, makespan_s):
     return out
 
 
-def run_served(pools, sched, bary, device=0, hbm_budget_bytes=40 << 30, tick_us=150):
+def run_served(pools, sched, bary, device=0, hbm_budget_bytes=40 << 30, tick_us=75, ticks_in_flight=None,
+               trace=False):
     from .serving import Server
-    srv = Server(device=device, hbm_budget_bytes=hbm_budget_bytes, tick_us=tick_us)
+    srv = Server(device=device, hbm_budget_bytes=hbm_budget_bytes, tick_us=tick_us, ticks_in_flight=ticks_in_flight)
     try:
         env_ids = {k: [srv.add_envmap(e) for e in v] for k, v in pools.envs.items()}
         mesh_ids = [srv.add_mesh(f, b) for f, b in pools.meshes]
@@ -123,16 +124,32 @@ def run_served(pools, sched, bary, device=0, hbm_budget_bytes=40 << 30, tick_us=
                                  nearest_triangle_id=pt["tri"][:P], barycentric_coord=bary[i],
                                  backward=r["backward"], grad_shading=pt["grad_shading"][:P],
                                  grad_diffuse_shading=pt["grad_diffuse_shading"][:P], outputs=outs)
-        srv.drain(600)
+        srv.drain(120)
         srv.poll(len(sched) + 16)
         stats = srv.stats()
     finally:
         srv.close()
+    bad = [q.status for q in reqs if q.status != 0]
+    if bad:
+        raise RuntimeError(f"{len(bad)} served requests failed (status {bad[0]})")
     # latency from the arrival time (submit happened at the arrival, to within the spin loop)
     lat = [(q.done[2] - q.done[0]) * 1e-9 for q in reqs]
     first = min(q.done[0] for q in reqs)
     last = max(q.done[2] for q in reqs)
     out = _summarize(lat, sched, (last - first) * 1e-9)
+    cls = [i for i, r in enumerate(sched) if 50000 <= r["P"] <= 100000 and r["res"] == (16, 32)]
+    if cls:
+        # where the class's time goes: wait for memory, upload, ordering, compute, download (p50 / p99, ms)
+        st = [reqs[i].stages for i in cls]
+        parts = {"admit": [x["admit"] - x["submit"] for x in st], "upload": [x["uploaded"] - x["admit"] for x in st],
+                 "order": [x["ready"] - x["uploaded"] for x in st],
+                 "compute": [x["computed"] - x["ready"] for x in st], "download": [x["done"] - x["computed"] for x in st]}
+        out["class_50k_100k_16x32"]["stages_ms"] = {
+            k: [float(np.percentile(v, 50)) * 1e-6, float(np.percentile(v, 99)) * 1e-6] for k, v in parts.items()}
+    if trace:  # per request: points, texels, visibility, backward, then its stage times in ns
+        keys = ("submit", "admit", "uploaded", "ready", "computed", "done")
+        out["trace"] = [[r["P"], r["res"][0] * r["res"][1], int(r["vis"]), int(r["backward"])] +
+                        [q.stages[k] for k in keys] for r, q in zip(sched, reqs)]
     out["ticks"] = stats["ticks"]
     out["items_per_tick"] = stats["items"] / max(stats["ticks"], 1)
     out["peak_arena_gb"] = stats["peak_arena_bytes"] / 2**30
@@ -188,14 +205,15 @@ def run_serial_plain(pools, sched, bary, device=0):
     return _summarize(lat, sched, makespan)
 
 
-def run(n=2000, rate=5000.0, tick_us=150, serial=True, hbm_budget_bytes=40 << 30, seed=7):
+def run(n=2000, rate=5000.0, tick_us=75, serial=True, hbm_budget_bytes=40 << 30, seed=7, ticks_in_flight=None):
     """Both arms on one arrival schedule; returns {"served": ..., "serial_plain": ...}."""
     pools = Pools()
     sched = make_schedule(n=n, rate=rate, seed=seed)
     bary = prepare_barycentrics(pools, sched)
     res = {"workload": f"{n} requests, Poisson {rate:.0f}/s, P log-uniform [1k, 500k], 16x32|32x64 env, "
-                       "visibility 50%, backward 30%", "tick_us": tick_us}
-    res["served"] = run_served(pools, sched, bary, hbm_budget_bytes=hbm_budget_bytes, tick_us=tick_us)
+                       "visibility 50%, backward 30%", "tick_us": tick_us, "ticks_in_flight": ticks_in_flight}
+    res["served"] = run_served(pools, sched, bary, hbm_budget_bytes=hbm_budget_bytes, tick_us=tick_us,
+                               ticks_in_flight=ticks_in_flight)
     if serial:
         res["serial_plain"] = run_serial_plain(pools, sched, bary)
     return res
@@ -207,7 +225,9 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=2000)
     ap.add_argument("--rate", type=float, default=5000.0)
-    ap.add_argument("--tick-us", type=int, default=150)
+    ap.add_argument("--tick-us", type=int, default=75)
+    ap.add_argument("--ticks-in-flight", type=int, default=None)
     ap.add_argument("--no-serial", action="store_true")
     a = ap.parse_args()
-    print(json.dumps(run(n=a.n, rate=a.rate, tick_us=a.tick_us, serial=not a.no_serial)))
+    print(json.dumps(run(n=a.n, rate=a.rate, tick_us=a.tick_us, serial=not a.no_serial,
+                         ticks_in_flight=a.ticks_in_flight)))

@@ -33,7 +33,9 @@ class _Request(ctypes.Structure):
 
 class _Done(ctypes.Structure):
     _fields_ = [("ticket", ctypes.c_int64), ("t_submit_ns", ctypes.c_int64), ("t_admit_ns", ctypes.c_int64),
-                ("t_done_ns", ctypes.c_int64), ("status", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("t_uploaded_ns", ctypes.c_int64), ("t_ready_ns", ctypes.c_int64), ("t_computed_ns", ctypes.c_int64),
+                ("t_done_ns", ctypes.c_int64),
+                ("status", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -61,8 +63,10 @@ def _load():
         L.des_server_drain.argtypes = [_vp, ctypes.c_int]
         L.des_server_stats.argtypes = [_vp, ctypes.POINTER(_Stats)]
         L.des_server_destroy.argtypes = [_vp]
+        L.des_server_set_ticks_in_flight.argtypes = [_vp, ctypes.c_int]
         for f in ("des_server_create", "des_server_add_envmap", "des_server_add_mesh", "des_server_submit",
-                  "des_server_poll", "des_server_drain", "des_server_stats", "des_server_destroy"):
+                  "des_server_poll", "des_server_drain", "des_server_stats", "des_server_destroy",
+                  "des_server_set_ticks_in_flight"):
             getattr(L, f).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -93,16 +97,20 @@ class Request:
         self._inputs = inputs
         self.outputs = outputs
         self.backward = backward
-        self.done = None  # (t_submit_ns, t_admit_ns, t_done_ns) once finished
+        self.done = None    # (t_submit_ns, t_admit_ns, t_done_ns) once finished
+        self.stages = None  # dict of every stage time (ns since server creation) once finished
+        self.status = None  # 0 (DES_OK) once finished successfully, else the des_status code
 
 
 class Server:
-    def __init__(self, device=0, hbm_budget_bytes=40 << 30, tick_us=150):
+    def __init__(self, device=0, hbm_budget_bytes=40 << 30, tick_us=150, ticks_in_flight=None):
         self._L = _load()
         h = _vp()
         _check(self._L.des_server_create(int(device), int(hbm_budget_bytes), int(tick_us), ctypes.byref(h)),
                "des_server_create")
         self._h = h
+        if ticks_in_flight is not None:
+            _check(self._L.des_server_set_ticks_in_flight(h, int(ticks_in_flight)), "des_server_set_ticks_in_flight")
         self._envs = {}
         self._requests = {}
 
@@ -171,7 +179,11 @@ class Server:
             d = buf[i]
             req = self._requests.pop(d.ticket, None)
             if req is not None:
+                req.status = d.status
                 req.done = (d.t_submit_ns, d.t_admit_ns, d.t_done_ns)
+                req.stages = {"submit": d.t_submit_ns, "admit": d.t_admit_ns, "uploaded": d.t_uploaded_ns,
+                              "ready": d.t_ready_ns,
+                              "computed": d.t_computed_ns, "done": d.t_done_ns}
                 out.append(req)
         return out
 

@@ -170,14 +170,17 @@ typedef struct des_serve_request {
 
 typedef struct des_serve_done {
   int64_t ticket;
-  int64_t t_submit_ns, t_admit_ns, t_done_ns; /* steady clock, relative to server creation */
+  /* steady clock, relative to server creation: submitted, admitted (memory reserved), inputs on
+   * the device, points ordered (ready to shade), last tile computed, outputs in host memory */
+  int64_t t_submit_ns, t_admit_ns, t_uploaded_ns, t_ready_ns, t_computed_ns, t_done_ns;
   int32_t status;
   int32_t pad;
 } des_serve_done;
 
 typedef struct des_serve_stats {
   int64_t submitted, completed, ticks, items, peak_arena_bytes;
-  int32_t device_error; /* workspace error word of the batch kernel (bit 0: bad mesh index) */
+  int32_t device_error; /* error word of the batch kernel: 1 bad mesh index, 4 malformed work item,
+                           8 bad permutation entry; 16 marks a tick that ran without its graph */
   int32_t pad;
 } des_serve_stats;
 
@@ -190,12 +193,16 @@ int des_server_add_envmap(des_server* s, int32_t H, int32_t W, const float* envm
 /* Registers a resident mesh: faces (3 x N_face) and visibility words (N_slot x N_vertex). */
 int des_server_add_mesh(des_server* s, int32_t N_face, int32_t N_vertex, int32_t N_slot,
                         const int32_t* face_vertex_list, const int32_t* visibility, int32_t* mesh_id);
-/* Queues a request; returns immediately with its ticket. */
+/* Queues a request; returns immediately with its ticket.  After a CUDA error the server fails every
+ * outstanding request (status DES_ERR_CUDA in des_serve_done) and refuses new ones. */
 int des_server_submit(des_server* s, const des_serve_request* req, int64_t* ticket);
 /* Moves up to max_items finished requests (outputs already in host memory) into out[]. */
 int des_server_poll(des_server* s, des_serve_done* out, int max_items, int* count);
 /* Waits until every submitted request has finished (DES_ERR_TIMEOUT after timeout_ms). */
 int des_server_drain(des_server* s, int timeout_ms);
+/* How many ticks may be queued on the GPU at once (1..4, default 3): more overlaps consecutive
+ * ticks better, fewer lets a newly arrived request start sooner. */
+int des_server_set_ticks_in_flight(des_server* s, int n);
 int des_server_stats(des_server* s, des_serve_stats* out);
 /* Finishes queued work and frees the server. */
 int des_server_destroy(des_server* s);

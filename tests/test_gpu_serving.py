@@ -123,6 +123,7 @@ def test_same_result_alone_and_in_the_mix(setup):
     srv.drain(120)
     done = srv.poll()
     assert mixed.done is not None and all(o.done is not None for o in others), len(done)
+    assert mixed.status == 0 and all(o.status == 0 for o in others)
     _compare(mixed.outputs, alone.outputs, "mix-vs-alone", exact=True)
     assert_close_grad(mixed.outputs["g_envmap"], alone.outputs["g_envmap"], "mix-vs-alone:g_envmap")
     want = _plain(des, inp, tri, bary, faces, vis_bits, envs[(16, 32)], True, True)
