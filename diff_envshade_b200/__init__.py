@@ -34,6 +34,13 @@ from ._C import (  # noqa: E402,F401  reference operator surface
     bruteforce_specular_shader_backward2,
     bruteforce_specularvisibility_shader_forward2,
     bruteforce_specularvisibility_shader_backward2,
+    get_nearest_mesh_points_forward,
+    get_nearest_mesh_points_backward,
+    get_uv_of_triangle_forward,
+    get_uv_of_triangle_backward,
+    extract_bitfield_forward,
+    sample_envmap_forward,
+    blur_envmap_forward,
     texel_table,
     workspace_bytes,
     set_timing_events,

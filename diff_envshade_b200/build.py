@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_LIB = os.path.join(PKG, "libdes_b200.so")
 CUDA_SOURCES = ["des_shade.cu", "des_capi.cu"]
-EXTRA_CUDA_SOURCES = ["des_noalloc.cu", "des_multienv.cu", "des_serve.cu"]  # built when present
+EXTRA_CUDA_SOURCES = ["des_noalloc.cu", "des_multienv.cu", "des_serve.cu", "des_mesh.cu", "des_envtools.cu"]  # built when present
 
 
 def ext_path():

@@ -438,6 +438,140 @@ int64_t workspace_bytes(int64_t P, int64_t H, int64_t W, int64_t flags, bool bac
   return (int64_t)des_shade_workspace_bytes(P, (int)H, (int)W, (unsigned)flags, backward ? 1 : 0, (int)device);
 }
 
+// ---- mesh-side helpers (reference etc.cu) ----
+
+void raise_error_word(const Tensor& err, const char* what) {
+  if (!check_indices_enabled()) return;
+  const int v = err.item<int>();
+  TORCH_CHECK(v == 0, what, ": a query had no candidate face or an id was out of range (error word ", v, ")");
+}
+
+Tensor get_uv_of_triangle_forward(const Tensor& triangles, const Tensor& query_pos) {
+  check_f32(triangles, "triangles");
+  check_f32(query_pos, "query_pos");
+  const int64_t P = query_pos.size(0);
+  TORCH_CHECK(query_pos.dim() == 2 && query_pos.size(1) == 3, "query_pos must have shape [P, 3]");
+  TORCH_CHECK(triangles.numel() == 9 * P, "triangles must have shape [P, 3, 3]");
+  const at::cuda::OptionalCUDAGuard guard(device_of(query_pos));
+  Tensor out = torch::empty({P, 3}, query_pos.options());
+  raise_status(des_get_uv_of_triangle_forward(P, triangles.data_ptr<float>(), query_pos.data_ptr<float>(),
+                                              out.data_ptr<float>(), cur_stream()));
+  return out;
+}
+
+Tensor get_uv_of_triangle_backward(const Tensor& triangles, const Tensor& query_pos,
+                                   const Tensor& grad_barycentric_coord) {
+  check_f32(triangles, "triangles");
+  check_f32(query_pos, "query_pos");
+  check_f32(grad_barycentric_coord, "grad_barycentric_coord");
+  const int64_t P = query_pos.size(0);
+  TORCH_CHECK(query_pos.dim() == 2 && query_pos.size(1) == 3, "query_pos must have shape [P, 3]");
+  TORCH_CHECK(triangles.numel() == 9 * P, "triangles must have shape [P, 3, 3]");
+  TORCH_CHECK(grad_barycentric_coord.numel() == 3 * P, "grad_barycentric_coord must have shape [P, 3]");
+  const at::cuda::OptionalCUDAGuard guard(device_of(query_pos));
+  Tensor out = torch::empty({P, 3}, query_pos.options());
+  raise_status(des_get_uv_of_triangle_backward(P, triangles.data_ptr<float>(), query_pos.data_ptr<float>(),
+                                               grad_barycentric_coord.data_ptr<float>(), out.data_ptr<float>(),
+                                               cur_stream()));
+  return out;
+}
+
+std::vector<Tensor> get_nearest_mesh_points_forward(const Tensor& adjacency_head, const Tensor& adjacency_list,
+                                                    const Tensor& face_vertex_list, const Tensor& vertex_pos,
+                                                    const Tensor& query_pos, const Tensor& idxs) {
+  check_i32(adjacency_head, "adjacency_head");
+  check_i32(adjacency_list, "adjacency_list");
+  check_i32(face_vertex_list, "face_vertex_list");
+  check_f32(vertex_pos, "vertex_pos");
+  check_f32(query_pos, "query_pos");
+  check_i64(idxs, "idxs");
+  TORCH_CHECK(adjacency_head.dim() == 2 && adjacency_head.size(0) == 2, "adjacency_head must have shape [2, N_vertex]");
+  TORCH_CHECK(face_vertex_list.dim() == 2 && face_vertex_list.size(0) == 3, "face_vertex_list must have shape [3, N_face]");
+  const int64_t N_vertex = adjacency_head.size(1), N_face = face_vertex_list.size(1), P = query_pos.size(1);
+  TORCH_CHECK(vertex_pos.dim() == 2 && vertex_pos.size(0) == 3 && vertex_pos.size(1) == N_vertex,
+              "vertex_pos must have shape [3, N_vertex]");
+  TORCH_CHECK(query_pos.dim() == 2 && query_pos.size(0) == 3, "query_pos must have shape [3, P]");
+  TORCH_CHECK(idxs.dim() == 2 && idxs.size(0) == P, "idxs must have shape [P, K]");
+  const int64_t K = idxs.size(1);
+  const at::cuda::OptionalCUDAGuard guard(device_of(query_pos));
+  Tensor tri = torch::empty({P}, idxs.options());
+  Tensor bary = torch::empty({3, P}, query_pos.options());
+  Tensor err = torch::zeros({1}, adjacency_head.options());
+  raise_status(des_get_nearest_mesh_points_forward(
+      (int32_t)N_vertex, (int32_t)N_face, P, (int32_t)K, adjacency_list.numel(), adjacency_head.data_ptr<int32_t>(),
+      adjacency_list.data_ptr<int32_t>(), face_vertex_list.data_ptr<int32_t>(), vertex_pos.data_ptr<float>(),
+      query_pos.data_ptr<float>(), idxs.data_ptr<int64_t>(), tri.data_ptr<int64_t>(), bary.data_ptr<float>(),
+      reinterpret_cast<unsigned*>(err.data_ptr<int32_t>()), cur_stream()));
+  raise_error_word(err, "get_nearest_mesh_points_forward");
+  return {tri, bary};
+}
+
+Tensor get_nearest_mesh_points_backward(const Tensor& face_vertex_list, const Tensor& vertex_pos,
+                                        const Tensor& query_pos, const Tensor& nearest_triangle_id,
+                                        const Tensor& grad_barycentric_coord) {
+  check_i32(face_vertex_list, "face_vertex_list");
+  check_f32(vertex_pos, "vertex_pos");
+  check_f32(query_pos, "query_pos");
+  check_i64(nearest_triangle_id, "nearest_triangle_id");
+  check_f32(grad_barycentric_coord, "grad_barycentric_coord");
+  const int64_t N_vertex = vertex_pos.size(1), N_face = face_vertex_list.size(1), P = query_pos.size(1);
+  TORCH_CHECK(query_pos.dim() == 2 && query_pos.size(0) == 3, "query_pos must have shape [3, P]");
+  TORCH_CHECK(nearest_triangle_id.numel() == P, "nearest_triangle_id must have P entries");
+  TORCH_CHECK(grad_barycentric_coord.numel() == 3 * P, "grad_barycentric_coord must have shape [3, P]");
+  const at::cuda::OptionalCUDAGuard guard(device_of(query_pos));
+  Tensor out = torch::empty({3, P}, query_pos.options());
+  Tensor err = torch::zeros({1}, face_vertex_list.options());
+  raise_status(des_get_nearest_mesh_points_backward(
+      (int32_t)N_vertex, (int32_t)N_face, P, face_vertex_list.data_ptr<int32_t>(), vertex_pos.data_ptr<float>(),
+      query_pos.data_ptr<float>(), nearest_triangle_id.data_ptr<int64_t>(), grad_barycentric_coord.data_ptr<float>(),
+      out.data_ptr<float>(), reinterpret_cast<unsigned*>(err.data_ptr<int32_t>()), cur_stream()));
+  raise_error_word(err, "get_nearest_mesh_points_backward");
+  return out;
+}
+
+Tensor extract_bitfield_forward(const Tensor& bitfield, int64_t N_bit, int64_t i_start, int64_t i_end) {
+  check_i32(bitfield, "bitfield");
+  TORCH_CHECK(bitfield.dim() == 2, "bitfield must have shape [N_slot, N]");
+  const int64_t N_slot = bitfield.size(0), N = bitfield.size(1);
+  TORCH_CHECK(N_bit >= 0 && N_bit <= 32 * N_slot, "N_bit must be in [0, 32 * N_slot]");
+  TORCH_CHECK(0 <= i_start && i_start <= i_end && i_end <= N, "need 0 <= i_start <= i_end <= N");
+  const at::cuda::OptionalCUDAGuard guard(device_of(bitfield));
+  Tensor out = torch::empty({i_end - i_start, N_bit}, bitfield.options().dtype(torch::kFloat));
+  raise_status(des_extract_bitfield_forward((int32_t)N_slot, (int32_t)N, (int32_t)N_bit, (int32_t)i_start,
+                                            (int32_t)i_end, bitfield.data_ptr<int32_t>(), out.data_ptr<float>(),
+                                            cur_stream()));
+  return out;
+}
+
+// ---- env-map preprocessing (reference etc.cu) ----
+
+Tensor sample_envmap_forward(const Tensor& query_point, const Tensor& envmap) {
+  check_f32(query_point, "query_point");
+  check_f32(envmap, "envmap");
+  TORCH_CHECK(query_point.dim() == 2 && query_point.size(0) == 3, "query_point must have shape [3, P]");
+  TORCH_CHECK(envmap.dim() == 3, "envmap must have shape [C, H, W]");
+  const int64_t P = query_point.size(1), C = envmap.size(0);
+  const at::cuda::OptionalCUDAGuard guard(device_of(envmap));
+  Tensor out = torch::empty({C, P}, envmap.options());
+  raise_status(des_sample_envmap_forward(P, (int32_t)envmap.size(1), (int32_t)envmap.size(2), (int32_t)C,
+                                         query_point.data_ptr<float>(), envmap.data_ptr<float>(),
+                                         out.data_ptr<float>(), cur_stream()));
+  return out;
+}
+
+Tensor blur_envmap_forward(const Tensor& envmap, int64_t tar_H, int64_t tar_W, int64_t N_samples, double alpha) {
+  check_f32(envmap, "envmap");
+  TORCH_CHECK(envmap.dim() == 3, "envmap must have shape [C, H, W]");
+  TORCH_CHECK(tar_H >= 0 && tar_W >= 0 && N_samples > 0, "need tar_H, tar_W >= 0 and N_samples > 0");
+  const int64_t C = envmap.size(0);
+  const at::cuda::OptionalCUDAGuard guard(device_of(envmap));
+  Tensor out = torch::empty({C, tar_H, tar_W}, envmap.options());
+  raise_status(des_blur_envmap_forward((int32_t)envmap.size(1), (int32_t)envmap.size(2), (int32_t)C, (int32_t)tar_H,
+                                       (int32_t)tar_W, (int32_t)N_samples, (float)alpha, envmap.data_ptr<float>(),
+                                       out.data_ptr<float>(), cur_stream()));
+  return out;
+}
+
 }  // namespace
 
 PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
@@ -452,6 +586,13 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("bruteforce_specular_shader_backward2", &bruteforce_specular_shader_backward2, "bruteforce specular shader backward2 (CUDA)");
   m.def("bruteforce_specularvisibility_shader_forward2", &bruteforce_specularvisibility_shader_forward2, "bruteforce specular visibility shader forward2 (CUDA)");
   m.def("bruteforce_specularvisibility_shader_backward2", &bruteforce_specularvisibility_shader_backward2, "bruteforce specular visibility shader backward2 (CUDA)");
+  m.def("get_nearest_mesh_points_forward", &get_nearest_mesh_points_forward, "get nearest mesh points forward (CUDA)");
+  m.def("get_nearest_mesh_points_backward", &get_nearest_mesh_points_backward, "get nearest mesh points backward (CUDA)");
+  m.def("get_uv_of_triangle_forward", &get_uv_of_triangle_forward, "get uv of triangle forward (CUDA)");
+  m.def("get_uv_of_triangle_backward", &get_uv_of_triangle_backward, "get uv of triangle backward (CUDA)");
+  m.def("extract_bitfield_forward", &extract_bitfield_forward, "extract bitfield to float forward (CUDA)");
+  m.def("blur_envmap_forward", &blur_envmap_forward, "blur envmap forward (CUDA)");
+  m.def("sample_envmap_forward", &sample_envmap_forward, "sample envmap forward (CUDA)");
   m.def("texel_table", &texel_table, "rotated texel table [H*W, 4] = (x, y, z, d_omega)");
   m.def("relight_multienv", &relight_multienv, "forward shading under K env maps on tcgen05 -> [P, K, 3]",
         py::arg("normal"), py::arg("view_dir"), py::arg("albedo"), py::arg("specular_albedo"), py::arg("roughness"),

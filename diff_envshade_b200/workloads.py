@@ -16,6 +16,7 @@ barycentrics (1,0,0), so each point's visibility is exactly its own bits) and ``
 barycentric interpolation.  All draws use a CPU ``torch.Generator`` so the same seed gives the
 same tensors on every machine.
 """
+import math
 from dataclasses import dataclass, field
 from typing import Optional
 
@@ -168,3 +169,60 @@ def make_config(name, **overrides):
     c.update(overrides)
     return make_inputs(c["P"], c["H"], c["W"], c["seed"], sigma=c["sigma"], rough=c["rough"], vis_p=c["vis_p"],
                        env_count=c.get("K", 1))
+
+
+# ---- mesh inputs of the visibility-gather helpers (get_nearest_mesh_points / get_uv_of_triangle) ----
+
+def make_sphere_mesh(n_lat, n_lon, seed, jitter=0.01):
+    """A closed UV sphere of radius 1 with jittered vertices: vertex_pos [3, N_vertex] float32,
+    face_vertex_list [3, N_face] int32 (two poles + n_lat rings of n_lon vertices)."""
+    g = torch.Generator().manual_seed(seed)
+    th = (torch.arange(1, n_lat + 1, dtype=torch.float64) / (n_lat + 1)) * math.pi
+    ph = torch.arange(n_lon, dtype=torch.float64) / n_lon * 2 * math.pi
+    T, Ph = torch.meshgrid(th, ph, indexing="ij")
+    ring = torch.stack([torch.sin(T) * torch.cos(Ph), torch.cos(T), torch.sin(T) * torch.sin(Ph)], 0).reshape(3, -1)
+    pos = torch.cat([torch.tensor([[0.0], [1.0], [0.0]], dtype=torch.float64), ring,
+                     torch.tensor([[0.0], [-1.0], [0.0]], dtype=torch.float64)], 1)
+    pos = pos + jitter * torch.randn(pos.shape, generator=g, dtype=torch.float64)
+    top, bot = 0, 1 + n_lat * n_lon
+    vid = lambda i, j: 1 + i * n_lon + (j % n_lon)  # noqa: E731
+    faces = []
+    for j in range(n_lon):
+        faces.append((top, vid(0, j + 1), vid(0, j)))
+        faces.append((bot, vid(n_lat - 1, j), vid(n_lat - 1, j + 1)))
+    for i in range(n_lat - 1):
+        for j in range(n_lon):
+            a, b, c, d = vid(i, j), vid(i, j + 1), vid(i + 1, j), vid(i + 1, j + 1)
+            faces.append((a, b, c))
+            faces.append((b, d, c))
+    f = torch.tensor(faces, dtype=torch.int32).T.contiguous()
+    return pos.float().contiguous(), f
+
+
+def vertex_adjacency(face_vertex_list, N_vertex):
+    """adjacency_head [2, N_vertex] int32 (faces per vertex; inclusive prefix sum of the counts) and
+    adjacency_list int32 (face ids per vertex, ascending), the layout the reference's
+    get_nearest_mesh_points_forward reads."""
+    f = face_vertex_list.long()
+    N_face = f.shape[1]
+    verts = f.reshape(-1)
+    fid = torch.arange(N_face).repeat(3)
+    order = torch.argsort(verts * N_face + fid)
+    lst = fid[order].to(torch.int32)
+    count = torch.bincount(verts, minlength=N_vertex).to(torch.int32)
+    head = torch.stack([count, torch.cumsum(count, 0).to(torch.int32)], 0).contiguous()
+    return head, lst.contiguous()
+
+
+def make_mesh_queries(vertex_pos, P, K, seed, spread=0.05, device="cpu"):
+    """Query points near the mesh surface [3, P] and their K nearest vertices [P, K] int64."""
+    g = torch.Generator().manual_seed(seed)
+    N_vertex = vertex_pos.shape[1]
+    base = torch.randint(0, N_vertex, (P,), generator=g)
+    q = vertex_pos[:, base] + spread * torch.randn(3, P, generator=g)
+    qd, vd = q.to(device), vertex_pos.to(device)
+    idx = []
+    for s in range(0, P, 4096):  # brute-force kNN in blocks
+        d = torch.cdist(qd[:, s:s + 4096].T.double(), vd.T.double())
+        idx.append(torch.topk(d, K, dim=1, largest=False).indices.cpu())
+    return q.contiguous(), torch.cat(idx, 0).to(torch.int64).contiguous()

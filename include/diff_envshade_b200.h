@@ -207,6 +207,58 @@ int des_server_stats(des_server* s, des_serve_stats* out);
 /* Finishes queued work and frees the server. */
 int des_server_destroy(des_server* s);
 
+/* ---------------------------------------------------------------------------------------
+ * Mesh-side helpers of the visibility path (reference etc.cu)
+ * ------------------------------------------------------------------------------------- */
+
+/* barycentric_coord[P x 3] = (1 - s - t, s, t) of the point of triangle p closest to query_pos[p];
+ * triangles: P x 3 vertices x 3 floats.  Replaces get_uv_of_triangle_forward (etc.cu:1218). */
+int des_get_uv_of_triangle_forward(int64_t P, const float* triangles, const float* query_pos,
+                                   float* barycentric_coord, des_stream_t stream);
+/* grad_query_pos[P x 3] from grad_barycentric_coord[P x 3].  Replaces get_uv_of_triangle_backward
+ * (etc.cu:1246). */
+int des_get_uv_of_triangle_backward(int64_t P, const float* triangles, const float* query_pos,
+                                    const float* grad_barycentric_coord, float* grad_query_pos, des_stream_t stream);
+/* Nearest point of the mesh to each query among the faces adjacent to its K nearest vertices
+ * (idxs[P x K], int64; negative entries are skipped).  adjacency_head[2 x N_vertex] holds per vertex
+ * its face count and the inclusive prefix sum of the counts into adjacency_list[N_adj].  Outputs
+ * nearest_triangle_id[P] (int64) and barycentric_coord[3 x P]; a query with no candidate face gets
+ * id -1 and zero coordinates and sets bit 0 of *error_word (optional, device memory).  Out-of-range
+ * ids in the inputs are skipped.  Replaces get_nearest_mesh_points_forward (etc.cu:1277). */
+int des_get_nearest_mesh_points_forward(int32_t N_vertex, int32_t N_face, int64_t P, int32_t K, int64_t N_adj,
+                                        const int32_t* adjacency_head, const int32_t* adjacency_list,
+                                        const int32_t* face_vertex_list, const float* vertex_pos,
+                                        const float* query_pos, const int64_t* idxs, int64_t* nearest_triangle_id,
+                                        float* barycentric_coord, unsigned* error_word, des_stream_t stream);
+/* grad_query_pos[3 x P] from grad_barycentric_coord[3 x P] through the closest-point map of each
+ * query's nearest triangle.  Replaces get_nearest_mesh_points_backward (etc.cu:1328), using the
+ * incoming gradient where the reference kernel reads its uninitialised output (etc.cu:884-888). */
+int des_get_nearest_mesh_points_backward(int32_t N_vertex, int32_t N_face, int64_t P, const int32_t* face_vertex_list,
+                                         const float* vertex_pos, const float* query_pos,
+                                         const int64_t* nearest_triangle_id, const float* grad_barycentric_coord,
+                                         float* grad_query_pos, unsigned* error_word, des_stream_t stream);
+/* out[(i_end - i_start) x N_bit] = bit k of the visibility words of point i (1.0f / 0.0f), from
+ * bitfield[N_slot x N] (texel k at bit k % 32 of slot k / 32).  Replaces extract_bitfield_forward
+ * (etc.cu:1044). */
+int des_extract_bitfield_forward(int32_t N_slot, int32_t N, int32_t N_bit, int32_t i_start, int32_t i_end,
+                                 const int32_t* bitfield, float* out, des_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Env-map preprocessing (reference etc.cu)
+ * ------------------------------------------------------------------------------------- */
+
+/* out[C x P] = bilinear lat-long lookup of envmap[C x H x W] in the directions query_point[3 x P]
+ * (normalised here; columns wrap at the seam, rows clamp at the poles).  Replaces
+ * sample_envmap_forward (etc.cu:1145), which allocates 3 x P whatever C is. */
+int des_sample_envmap_forward(int64_t P, int32_t H, int32_t W, int32_t C, const float* query_point,
+                              const float* envmap, float* out, des_stream_t stream);
+/* out[C x tar_H x tar_W] = per output texel the mean of N_samples lookups of envmap[C x H x W] in
+ * directions drawn from the GGX distribution of roughness parameter alpha around the texel's
+ * direction (curand XORWOW, seed 0, one subsequence per texel, as the reference).  C is 3 or 4.
+ * Replaces blur_envmap_forward (etc.cu:1103). */
+int des_blur_envmap_forward(int32_t H, int32_t W, int32_t C, int32_t tar_H, int32_t tar_W, int32_t N_samples,
+                            float alpha, const float* envmap, float* out, des_stream_t stream);
+
 /* The rotated texel table the kernels integrate over, written to table_out[H*W x 4] as
  * (x, y, z, d_omega) per texel in memory order.  Bit-exact with the reference's per-pair
  * getLightDir / getDeltaOmega / rotation (bruteforce_shader.cu:124-147, 2174-2197). */

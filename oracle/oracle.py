@@ -14,6 +14,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "envshade_oracle.cpp")
+SRCS = [SRC, os.path.join(HERE, "mesh_oracle.cpp")]
 LIB = os.path.join(HERE, "libdes_oracle.so")
 
 DIFFUSE, SPECULAR, CLAMP, WHITE, V1ORDER = 1, 2, 4, 8, 16
@@ -29,10 +30,10 @@ OP_FLAGS = {
 
 
 def build(force=False):
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= os.path.getmtime(SRC):
+    if not force and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(s) for s in SRCS):
         return LIB
     tmp = LIB + ".tmp"
-    subprocess.check_call(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread", SRC, "-o", tmp])
+    subprocess.check_call(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread", *SRCS, "-o", tmp])
     os.replace(tmp, LIB)
     return LIB
 
@@ -57,6 +58,21 @@ def lib():
                 [P] * 4 + [ctypes.c_uint] + [P] * 8 + [ctypes.c_int]
         L.des_oracle_texel_table_f64.restype = None
         L.des_oracle_texel_table_f64.argtypes = [ctypes.c_int, ctypes.c_int, P, P]
+        i64 = ctypes.c_int64
+        L.des_oracle_uv_of_triangle_f64.restype = None
+        L.des_oracle_uv_of_triangle_f64.argtypes = [i64, P, P, P]
+        L.des_oracle_uv_of_triangle_backward_f64.restype = None
+        L.des_oracle_uv_of_triangle_backward_f64.argtypes = [i64, P, P, P, P]
+        for suf in ("f64", "f32"):
+            f = getattr(L, f"des_oracle_nearest_mesh_points_{suf}")
+            f.restype = i64
+            f.argtypes = [i64] * 5 + [P] * 8
+        L.des_oracle_nearest_mesh_points_backward_f64.restype = None
+        L.des_oracle_nearest_mesh_points_backward_f64.argtypes = [i64, i64, i64] + [P] * 6
+        L.des_oracle_extract_bitfield.restype = None
+        L.des_oracle_extract_bitfield.argtypes = [i64] * 4 + [P, P]
+        L.des_oracle_sample_envmap_f64.restype = None
+        L.des_oracle_sample_envmap_f64.argtypes = [i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]
         _lib = L
     return _lib
 
@@ -169,3 +185,69 @@ def flags_for(op, enable_diffuse=True, enable_specular=True):
     elif enable_specular and op != "diffuse":
         f |= SPECULAR
     return f
+
+
+# ---- mesh-side helpers and env-map sampling (mesh_oracle.cpp; reference etc.cu) ----
+
+def uv_of_triangle(triangles, query_pos):
+    """[P, 3, 3] triangles, [P, 3] queries -> [P, 3] barycentric (1 - s - t, s, t), FP64."""
+    tri = _np(triangles, np.float64).reshape(-1, 9)
+    q = _np(query_pos, np.float64).reshape(-1, 3)
+    out = np.zeros((q.shape[0], 3))
+    lib().des_oracle_uv_of_triangle_f64(q.shape[0], _ptr(tri), _ptr(q), _ptr(out))
+    return out
+
+
+def uv_of_triangle_backward(triangles, query_pos, grad_bary):
+    tri = _np(triangles, np.float64).reshape(-1, 9)
+    q = _np(query_pos, np.float64).reshape(-1, 3)
+    g = _np(grad_bary, np.float64).reshape(-1, 3)
+    out = np.zeros_like(q)
+    lib().des_oracle_uv_of_triangle_backward_f64(q.shape[0], _ptr(tri), _ptr(q), _ptr(g), _ptr(out))
+    return out
+
+
+def nearest_mesh_points(adjacency_head, adjacency_list, faces, vertex_pos, query_pos, idxs, dtype=np.float64):
+    """Returns (triangle id [P] int64, barycentric [3, P], number of queries without a face)."""
+    head = _np(adjacency_head, np.int32)
+    lst = _np(adjacency_list, np.int32)
+    f = _np(faces, np.int32)
+    vp = _np(vertex_pos, dtype)
+    q = _np(query_pos, dtype)
+    ix = _np(idxs, np.int64)
+    P, K = q.shape[1], ix.shape[1]
+    tri = np.zeros(P, dtype=np.int64)
+    bary = np.zeros((3, P), dtype=dtype)
+    fn = lib().des_oracle_nearest_mesh_points_f64 if dtype == np.float64 else lib().des_oracle_nearest_mesh_points_f32
+    missing = fn(head.shape[1], f.shape[1], P, K, lst.size, _ptr(head), _ptr(lst), _ptr(f), _ptr(vp), _ptr(q),
+                 _ptr(ix), _ptr(tri), _ptr(bary))
+    return tri, bary, int(missing)
+
+
+def nearest_mesh_points_backward(faces, vertex_pos, query_pos, tri, grad_bary):
+    f = _np(faces, np.int32)
+    vp = _np(vertex_pos, np.float64)
+    q = _np(query_pos, np.float64)
+    t = _np(tri, np.int64)
+    g = _np(grad_bary, np.float64)
+    out = np.zeros_like(q)
+    lib().des_oracle_nearest_mesh_points_backward_f64(vp.shape[1], f.shape[1], q.shape[1], _ptr(f), _ptr(vp), _ptr(q),
+                                                      _ptr(t), _ptr(g), _ptr(out))
+    return out
+
+
+def extract_bitfield(bitfield, N_bit, i_start, i_end):
+    w = _np(bitfield, np.int32).view(np.uint32)
+    out = np.zeros((i_end - i_start, N_bit), dtype=np.float32)
+    lib().des_oracle_extract_bitfield(w.shape[1], N_bit, i_start, i_end, _ptr(w), _ptr(out))
+    return out
+
+
+def sample_envmap(query_point, envmap):
+    """[3, P] directions, [C, H, W] env -> [C, P] bilinear lat-long samples, FP64."""
+    q = _np(query_point, np.float64)
+    env = _np(envmap, np.float64)
+    C, H, W = env.shape
+    out = np.zeros((C, q.shape[1]))
+    lib().des_oracle_sample_envmap_f64(q.shape[1], H, W, C, _ptr(q), _ptr(env), _ptr(out))
+    return out

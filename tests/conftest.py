@@ -109,4 +109,9 @@ def reference_ext():
 
 
 def golden_files(pattern="*.npz"):
-    return sorted(glob.glob(os.path.join(GOLDEN, pattern)))
+    """Fixture files matching pattern; the etc_*.npz fixtures of the mesh and env-map helpers are
+    listed only when the pattern names them."""
+    files = sorted(glob.glob(os.path.join(GOLDEN, pattern)))
+    if not pattern.startswith("etc_"):
+        files = [f for f in files if not os.path.basename(f).startswith("etc_")]
+    return files

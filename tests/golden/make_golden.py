@@ -11,7 +11,11 @@ that each see exactly one texel through a one-hot visibility word, with axis-ali
 and unit radiance.  That output equals fl(fl(+-l_k / pi) * d_omega) for the texel's rotated
 direction component l_k, which pins the texel table bit-for-bit.
 
-Usage:  python tests/golden/make_golden.py --out tests/golden
+With ``--only-etc`` it writes only ``etc_*.npz``: the reference's mesh-side helpers
+(get_uv_of_triangle forward/backward, get_nearest_mesh_points forward), extract_bitfield,
+sample_envmap and blur_envmap on seeded inputs (the shading fixtures above are left as they are).
+
+Usage:  python tests/golden/make_golden.py --out tests/golden [--only-etc]
 """
 import argparse
 import glob
@@ -114,11 +118,16 @@ def table_probe_inputs(H, W, R):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    ap.add_argument("--only-etc", action="store_true", help="write only the etc_*.npz helper fixtures")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     ref = load_reference()
     import diff_envshade_b200 as des
     from diff_envshade_b200 import workloads as wl
+
+    write_etc_fixtures(ref, a.out)
+    if a.only_etc:
+        return
 
     for name, (op, P, H, W, seed, layout, ed, es, rot, rough) in CASES.items():
         inp = wl.make_inputs(P, H, W, seed, rough=rough, vis_p=(0.7 if layout else None),
@@ -198,6 +207,60 @@ def table_probes(ref, H, W, R, one_hot_env):
         out["ref_white_novis"] = wn
     torch.cuda.synchronize()
     return out
+
+
+
+def write_etc_fixtures(ref, out_dir):
+    """Reference outputs of the mesh-side and env-map helpers (etc.cu) on seeded inputs."""
+    from diff_envshade_b200 import workloads as wl
+    g = torch.Generator().manual_seed(2024)
+    # get_uv_of_triangle: random triangles, queries around them (interior, edge and vertex regions)
+    P = 1024
+    tri = torch.randn(P, 3, 3, generator=g)
+    w = torch.rand(P, 3, generator=g) * 1.6 - 0.3
+    q = (w[:, :, None] * tri).sum(1) + 0.2 * torch.randn(P, 3, generator=g)
+    gb = torch.randn(P, 3, generator=g)
+    bary = ref.get_uv_of_triangle_forward(tri.cuda(), q.cuda())
+    gq = ref.get_uv_of_triangle_backward(tri.cuda(), q.cuda(), gb.cuda())
+    np.savez_compressed(os.path.join(out_dir, "etc_uv_of_triangle.npz"), triangles=tri.numpy(), query_pos=q.numpy(),
+                        grad_barycentric_coord=gb.numpy(), ref_barycentric_coord=bary.cpu().numpy(),
+                        ref_grad_query_pos=gq.cpu().numpy())
+    # get_nearest_mesh_points forward on a jittered sphere (the reference backward reads its own
+    # output buffer as the incoming gradient, so only the forward is a usable fixture)
+    pos, faces = wl.make_sphere_mesh(16, 32, seed=7)
+    head, lst = wl.vertex_adjacency(faces, pos.shape[1])
+    qp, idx = wl.make_mesh_queries(pos, 2048, 4, seed=8)
+    # the reference kernel traps (ends the CUDA context) when a query has no candidate face or more
+    # than 128 distinct ones: check on the CPU that every query has 1..128 before running it
+    n, end = head[0].numpy(), head[1].numpy()
+    cand = [len({f for v in row for f in lst.numpy()[end[v] - n[v]:end[v]]}) for row in idx.numpy()]
+    assert 1 <= min(cand) and max(cand) <= 128, (min(cand), max(cand))
+    tri_id, nb = ref.get_nearest_mesh_points_forward(head.cuda(), lst.cuda(), faces.cuda(), pos.cuda(), qp.cuda(),
+                                                     idx.cuda())
+    np.savez_compressed(os.path.join(out_dir, "etc_nearest_mesh_points.npz"), adjacency_head=head.numpy(),
+                        adjacency_list=lst.numpy(), face_vertex_list=faces.numpy(), vertex_pos=pos.numpy(),
+                        query_pos=qp.numpy(), idxs=idx.numpy(), ref_nearest_triangle_id=tri_id.cpu().numpy(),
+                        ref_barycentric_coord=nb.cpu().numpy())
+    # extract_bitfield: ragged bit count, a window of points
+    words = torch.randint(-2 ** 31, 2 ** 31 - 1, (16, 300), generator=g, dtype=torch.int64).to(torch.int32)
+    bits = ref.extract_bitfield_forward(words.cuda(), 500, 17, 250)
+    np.savez_compressed(os.path.join(out_dir, "etc_extract_bitfield.npz"), bitfield=words.numpy(),
+                        meta=np.array([500, 17, 250]), ref_out=bits.cpu().numpy())
+    # sample_envmap: random directions (not normalised) on a lognormal 3 x 16 x 32 map
+    env = torch.exp(torch.randn(3, 16, 32, generator=g))
+    dirs = torch.randn(3, 2048, generator=g) * torch.rand(1, 2048, generator=g).add(0.5)
+    smp = ref.sample_envmap_forward(dirs.cuda(), env.cuda())
+    # blur_envmap: 3 x 16 x 32 -> 8 x 16, 64 samples, alpha 0.3; and 4 channels -> 4 x 8
+    blur = ref.blur_envmap_forward(env.cuda(), 8, 16, 64, 0.3)
+    env4 = torch.exp(torch.randn(4, 8, 16, generator=g))
+    blur4 = ref.blur_envmap_forward(env4.cuda(), 4, 8, 16, 0.7)
+    np.savez_compressed(os.path.join(out_dir, "etc_envmap_sampling.npz"), envmap=env.numpy(), query_point=dirs.numpy(),
+                        ref_sample=smp.cpu().numpy(), ref_blur=blur.cpu().numpy(), blur_args=np.array([8, 16, 64]),
+                        blur_alpha=np.array([0.3], dtype=np.float32), envmap4=env4.numpy(),
+                        ref_blur4=blur4.cpu().numpy(), blur4_args=np.array([4, 8, 16]),
+                        blur4_alpha=np.array([0.7], dtype=np.float32))
+    torch.cuda.synchronize()
+    print("wrote etc fixtures")
 
 
 if __name__ == "__main__":
