@@ -28,6 +28,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "des_internal.h"
 #include "des_math.cuh"
@@ -184,8 +185,8 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_
   const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
   const float2 hf = __bfloat1622float2(h);
   const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
-  hi = *reinterpret_cast<const uint32_t*>(&h);
-  lo = *reinterpret_cast<const uint32_t*>(&l);
+  memcpy(&hi, &h, sizeof(hi));  // bit copies, kept in registers
+  memcpy(&lo, &l, sizeof(lo));
 }
 
 // ---- radiance preparation ------------------------------------------------------------------
@@ -269,8 +270,8 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
     const bool need_view = SPEC || p.pt.clamp;
     uint32_t q = 0;
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
-      const int64_t pid = (int64_t)tile * kTileM + row;
-      const bool valid = pid < p.pt.P;
+      int64_t pid = (int64_t)tile * kTileM + row;
+      const bool valid = ordered_point(p.pt.perm, (int64_t)tile * kTileM + row, p.pt.P, p.pt.ctrl, pid);
       const PointGeom g = load_geom<VIS>(p.pt, pid, valid, need_view);
       SpecConst sc;
       if (SPEC) sc = spec_const(valid ? p.pt.rough[pid] : 0.f, g);
@@ -282,16 +283,20 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
           if (SPEC) spc[c] = p.pt.spec[3 * pid + c];
         }
       }
+      // visibility words of the next stage are loaded while this one is built
+      uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
+      if (VIS) load_vis_words(p.pt, g, valid, 0, n0, n1, n2);
       for (int st = 0; st < p.nst; ++st, ++q) {
         const uint32_t b = q & 1u, u = q >> 1;
         uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
         if (VIS) {
-          load_vis_words(p.pt, g, valid, st, w0, w1, w2);
-          w0 >>= 16 * half;
-          w1 >>= 16 * half;
-          w2 >>= 16 * half;
+          w0 = n0 >> (16 * half);
+          w1 = n1 >> (16 * half);
+          w2 = n2 >> (16 * half);
+          if (st + 1 < p.nst) load_vis_words(p.pt, g, valid, st + 1, n0, n1, n2);
         }
-        if (u > 0 && !mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err)) goto builders_done;
+        // the whole warp leaves together (the texel votes below need all 32 lanes)
+        if (u > 0 && !__all_sync(0xffffffffu, mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err))) goto builders_done;
         {
           const uint32_t abuf = a_base + b * (3 * 2 * kATile);
 #pragma unroll
@@ -305,6 +310,12 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
                 const int jl = j8 * 8 + jj + e;  // 0..15 within this thread's half stage
                 const int t = st * kStageT + half * 16 + jl;
                 const float4 A = s_tab[2 * t];
+                // texel below the horizon of the warp's 32 (ordered) points: zero weights
+                if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) {
+#pragma unroll
+                  for (int c = 0; c < 3; ++c) av[c][e] = 0.f;
+                  continue;
+                }
                 const float4 B = s_tab[2 * t + 1];
                 const float vis = VIS ? vis_weight(w0, w1, w2, 1u << jl, g.c0, g.c1, g.c2) : 1.f;
                 float wd, ws;
@@ -384,7 +395,8 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
       const uint32_t abuf = (uint32_t)i & 1u, au = (uint32_t)i >> 1;
       if (!mbar_wait(&acc_full[abuf], au & 1u, s_abort, err)) break;
       tc_fence_after();
-      const int64_t pid = (int64_t)tile * kTileM + row;
+      int64_t pid = 0;
+      const bool live = ordered_point(p.pt.perm, (int64_t)tile * kTileM + row, p.pt.P, p.pt.ctrl, pid);
       float* orow = p.out + pid * p.ldo + (int64_t)p.kbase * 3;
       for (int kb = 0; kb < p.kpad / 16; ++kb) {
         float v[3][16];
@@ -392,7 +404,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
         for (int c = 0; c < 3; ++c)
           tmem_ld16(tmem + (quarter * 32u << 16) + (abuf * 3u + (uint32_t)c) * (uint32_t)p.kpad + kb * 16, v[c]);
         tmem_wait_ld();
-        if (pid < p.pt.P) {
+        if (live) {
           const int k0 = kb * 16;
           if (p.vec_store && k0 + 16 <= p.kblock) {
             float4* o4 = reinterpret_cast<float4*>(orow + k0 * 3);
@@ -503,7 +515,10 @@ size_t relight_workspace_bytes(int64_t P, int H, int W, int K) {
   if (P < 0 || H <= 0 || W <= 0 || K <= 0) return 0;
   const int HWpad = (H * W + 31) / 32 * 32;
   const int kpad = kpad_of(std::min(K, relight::kEnvBlock));
-  return kCtrlBytes + align256((size_t)HWpad * 32) + align256((size_t)(HWpad / 32) * relight::bprep_stage_bytes(kpad));
+  size_t b = kCtrlBytes + align256((size_t)HWpad * 32) + align256((size_t)(HWpad / 32) * relight::bprep_stage_bytes(kpad));
+  if (P >= kSortMinP && P <= kSortMaxP)  // normal-direction ordering: permutation + its scratch
+    b += align256((size_t)P * 4) + align256(point_order_scratch_bytes(P));
+  return b;
 }
 
 int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigned flags, float* out, void* ws,
@@ -525,6 +540,8 @@ int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigne
   unsigned* ctrl = reinterpret_cast<unsigned*>(w);
   float4* table = reinterpret_cast<float4*>(w + kCtrlBytes);
   uint8_t* bprep = w + kCtrlBytes + align256((size_t)HWpad * 32);
+  const int kpad_max = kpad_of(std::min(K, relight::kEnvBlock));
+  uint8_t* order_area = bprep + align256((size_t)(HWpad / 32) * relight::bprep_stage_bytes(kpad_max));
 
   int st = launch_table(a.H, a.W, HWpad, a.light2obj_rotmat, envmaps, table, ctrl, stream);
   if (st != DES_OK) return st;
@@ -558,6 +575,15 @@ int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigne
   prm.nst = HWpad / relight::kStageT;
   prm.ntiles = (int)((a.P + relight::kTileM - 1) / relight::kTileM);
   prm.split = !(flags & DES_RELIGHT_BF16);
+  pt.perm = nullptr;
+  if (a.P >= kSortMinP && a.P <= kSortMaxP) {
+    // order the points by normal direction: each builder warp's 32 points then face the same way
+    // and texels below all of their horizons are skipped (per-point results unchanged)
+    int32_t* perm = reinterpret_cast<int32_t*>(order_area);
+    st = launch_point_order(a.normal, a.P, order_area + align256((size_t)a.P * 4), perm, stream);
+    if (st != DES_OK) return st;
+    pt.perm = perm;
+  }
 
   RelightFn k = pick_relight(diff, spec, vis);
   const int grid = std::max(1, std::min(prm.ntiles, sms));
