@@ -19,7 +19,8 @@ int validate(const des_shade_args* a, unsigned flags, bool backward, const void*
   if (a->C != 3) return DES_ERR_UNSUPPORTED;
   if (a->P < 0 || a->H <= 0 || a->W <= 0) return DES_ERR_INVALID_ARGUMENT;
   if ((int64_t)a->H * a->W > kMaxTexels) return DES_ERR_UNSUPPORTED;
-  if (flags & ~(unsigned)(DES_DIFFUSE | DES_SPECULAR | DES_CLAMP | DES_INPUT_ORDER)) return DES_ERR_INVALID_ARGUMENT;
+  if (flags & ~(unsigned)(DES_DIFFUSE | DES_SPECULAR | DES_CLAMP | DES_INPUT_ORDER | DES_COMPACT))
+    return DES_ERR_INVALID_ARGUMENT;
   if (a->envmap == nullptr || a->light2obj_rotmat == nullptr) return DES_ERR_INVALID_ARGUMENT;
   if (a->P == 0) return DES_OK;
   if (a->normal == nullptr || out0 == nullptr) return DES_ERR_INVALID_ARGUMENT;
@@ -80,7 +81,7 @@ size_t des_shade_workspace_bytes(int64_t P, int32_t H, int32_t W, unsigned flags
   int prev = 0;
   if (cudaGetDevice(&prev) != cudaSuccess) return 0;
   if (device != prev && cudaSetDevice(device) != cudaSuccess) return 0;
-  des::LaunchPlan lp = des::plan_launch(P, H, W, backward != 0, device);
+  des::LaunchPlan lp = des::plan_launch(P, H, W, backward != 0, device, (flags & DES_COMPACT) != 0);
   if (flags & DES_INPUT_ORDER) {
     lp.sort = false;
     lp.sort_chunks = 0;

@@ -89,7 +89,9 @@ struct ShadeCall {
   size_t workspace_bytes;
 };
 
-LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev);
+// compact: the plan with the smallest workspace: input order, and for the adjoint the widest CTAs
+// (fewest persistent CTAs, so fewest env-map gradient partials).
+LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev, bool compact = false);
 size_t workspace_bytes(const LaunchPlan& lp, bool backward, int grid);
 int shade_grid(const LaunchPlan& lp, unsigned flags, bool backward, bool vis);
 int launch_shade(const ShadeCall& call, des_stream_t stream);

@@ -10,9 +10,9 @@
 // Limits and behaviour:
 //  * the array is DES_SHADE_NOALLOC_SCRATCH_BYTES (4 MiB) and lives as long as the library is loaded:
 //    every GPU on which it is used keeps those 4 MiB until the process exits;
-//  * the points are shaded in input order when the array is too small for the normal-direction
-//    ordering (DES_INPUT_ORDER: same results, somewhat slower for large batches); a call whose
-//    des_shade_workspace_bytes(P, H, W, flags | DES_INPUT_ORDER, 1, device) exceeds the array is
+//  * when the array is too small for the default plan, the call runs in input order, and if need be
+//    with the compact plan (DES_COMPACT: fewest persistent CTAs; same results, slower); a call
+//    whose des_shade_workspace_bytes(P, H, W, flags | DES_COMPACT, 1, device) exceeds the array is
 //    rejected with DES_ERR_WORKSPACE before anything is launched (on a 148-SM B200 this admits any
 //    point count with env maps up to 16 x 32 texels, and larger maps only for small batches);
 //  * all calls share the one array and it keeps the previous call's contents: the launch path resets
@@ -63,7 +63,7 @@ extern "C" int des_shade_backward_noalloc(const des_shade_args* args, unsigned f
   if (args == nullptr) return DES_ERR_INVALID_ARGUMENT;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return DES_ERR_CUDA;
-  const size_t need = des_shade_workspace_bytes(args->P, args->H, args->W, flags | DES_INPUT_ORDER, 1, dev);
+  const size_t need = des_shade_workspace_bytes(args->P, args->H, args->W, flags | DES_COMPACT, 1, dev);
   if (need == 0) return args->C != 3 ? DES_ERR_UNSUPPORTED : DES_ERR_INVALID_ARGUMENT;
   if (need > sizeof(g_noalloc_scratch)) return DES_ERR_WORKSPACE;
   void* scratch = nullptr;

@@ -598,6 +598,7 @@ namespace {
 struct DeviceInfo {
   int sms = 0;
   int max_smem_optin = 0;
+  int smem_per_sm = 0;
 };
 
 DeviceInfo device_info(int dev) {
@@ -608,6 +609,7 @@ DeviceInfo device_info(int dev) {
   if (cache[dev].sms == 0) {
     cudaDeviceGetAttribute(&cache[dev].sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&cache[dev].max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&cache[dev].smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   }
   return cache[dev];
 }
@@ -671,7 +673,7 @@ inline int sort_row(const LaunchPlan& lp) { return (lp.sort_chunks + 3) / 4 * 4;
 
 }  // namespace
 
-LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev) {
+LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev, bool compact) {
   LaunchPlan lp{};
   const DeviceInfo di = device_info(dev);
   const int HW = H * W;
@@ -679,16 +681,39 @@ LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev) {
   lp.chunk = std::min(lp.HWpad, kChunk);
   lp.ntiles = (int)((P + 31) / 32);
   lp.env_in_smem = backward && (lp.HWpad <= kChunk);
-  // texel-split width: more warps per tile when there are few tiles to spread over the SMs
+  // texel-split width (warps per tile).  With few tiles, 16 warps share each tile.  Otherwise the
+  // width that keeps the most warps resident per SM, from the register bound of the kernel (128 per
+  // thread for the adjoint, 64 for the forward), its shared memory and the thread limit; on a tie
+  // the adjoint takes the narrowest CTA (more independent tiles in flight, smaller barrier groups)
+  // and the forward 8 warps (measured best at 16x32 maps).
   const int nslots = lp.chunk / 32;
-  int nw = (lp.ntiles >= 2 * std::max(di.sms, 1)) ? 8 : 16;
+  const int nacc = backward ? 15 : 6;
+  const int regs = backward ? 128 : 64;
+  auto smem_for = [&](int w) {
+    return (size_t)lp.chunk * 32 + (lp.env_in_smem ? (size_t)lp.chunk * 24 : 0) + (size_t)w * nacc * 32 * 4;
+  };
+  int nw = 16;
+  if (!(compact && backward) && lp.ntiles >= 2 * std::max(di.sms, 1) && di.smem_per_sm > 0) {
+    int best_warps = -1;
+    const int order[3] = {backward ? 4 : 8, backward ? 8 : 4, 16};
+    for (int w : order) {
+      if (w > nslots) continue;
+      const int by_regs = 65536 / (regs * 32 * w);
+      const int by_smem = (int)((size_t)di.smem_per_sm / (smem_for(w) + 1024));
+      const int by_threads = 2048 / (32 * w);
+      const int warps = w * std::min(by_regs, std::min(by_smem, by_threads));
+      if (warps > best_warps) {
+        best_warps = warps;
+        nw = w;
+      }
+    }
+  }
   while (nw > 1 && nw > nslots) nw >>= 1;
   lp.nw = nw;
-  const int nacc = backward ? 15 : 6;
-  lp.smem = (size_t)lp.chunk * 32 + (lp.env_in_smem ? (size_t)lp.chunk * 24 : 0) + (size_t)nw * nacc * 32 * 4;
+  lp.smem = smem_for(nw);
   lp.sms = di.sms;
   lp.max_smem = di.max_smem_optin;
-  lp.sort = P >= kSortMinP && P <= kSortMaxP;
+  lp.sort = !compact && P >= kSortMinP && P <= kSortMaxP;
   lp.sort_chunk = sort_chunk_for(P);
   lp.sort_chunks = lp.sort ? (int)((P + lp.sort_chunk - 1) / lp.sort_chunk) : 0;
   return lp;
@@ -741,20 +766,28 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   const bool vis = a.visibility != nullptr;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return DES_ERR_CUDA;
-  LaunchPlan lp = plan_launch(a.P, a.H, a.W, call.backward, dev);
+  const bool compact = (call.flags & DES_COMPACT) != 0;
+  LaunchPlan lp = plan_launch(a.P, a.H, a.W, call.backward, dev, compact);
   if (call.flags & DES_INPUT_ORDER) {
     lp.sort = false;
     lp.sort_chunks = 0;
   }
   if (lp.smem > (size_t)lp.max_smem) return DES_ERR_UNSUPPORTED;
-  const int grid = shade_grid(lp, call.flags, call.backward, vis);
+  int grid = shade_grid(lp, call.flags, call.backward, vis);
   if (grid <= 0) return DES_ERR_CUDA;
   size_t need = workspace_bytes(lp, call.backward, grid);
+  // A workspace sized for a smaller plan (e.g. the allocation-free entry point's static array):
+  // shade in input order, then with the compact plan -- same results, less scratch.
   if (lp.sort && call.workspace_bytes < need) {
-    // a workspace sized for input order (e.g. the allocation-free entry point's static array):
-    // shade in input order -- same results, no ordering scratch
     lp.sort = false;
     lp.sort_chunks = 0;
+    need = workspace_bytes(lp, call.backward, grid);
+  }
+  if (!compact && call.workspace_bytes < need) {
+    lp = plan_launch(a.P, a.H, a.W, call.backward, dev, true);
+    if (lp.smem > (size_t)lp.max_smem) return DES_ERR_UNSUPPORTED;
+    grid = shade_grid(lp, call.flags, call.backward, vis);
+    if (grid <= 0) return DES_ERR_CUDA;
     need = workspace_bytes(lp, call.backward, grid);
   }
   if (call.workspace == nullptr || call.workspace_bytes < need ||

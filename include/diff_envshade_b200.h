@@ -50,6 +50,12 @@ typedef enum des_status {
  * values bit for bit; the env-map gradient up to FP64 summation order).  Input order needs a
  * smaller workspace; a workspace too small for the ordering also falls back to input order. */
 #define DES_INPUT_ORDER 16u
+/* des_shade_*: the smallest workspace -- input order, and for the adjoint the widest CTAs (the
+ * fewest persistent CTAs, each of which keeps its own FP64 env-map gradient partial).  Slower.  The
+ * forward's outputs are the same bit for bit; the adjoint's agree to FP32 rounding (each point's
+ * texel sum is split over a different number of warps).  A workspace too small for the default
+ * plan also falls back to input order, then to this plan. */
+#define DES_COMPACT 32u
 
 /* All inputs of one shading call.  The visibility block is ignored when visibility == NULL. */
 typedef struct des_shade_args {
@@ -108,8 +114,8 @@ int des_shade_backward(const des_shade_args* args, unsigned flags, const float* 
  * reference).  Same inputs and outputs as des_shade_backward, no workspace argument: scratch comes
  * from a library-owned static device array of DES_SHADE_NOALLOC_SCRATCH_BYTES, held on every GPU
  * that uses it until the process exits.  Returns DES_ERR_WORKSPACE, without launching anything,
- * when des_shade_workspace_bytes(P, H, W, flags | DES_INPUT_ORDER, 1, device) exceeds that size
- * (a problem that fits only in input order runs in input order).  All calls share the
+ * when des_shade_workspace_bytes(P, H, W, flags | DES_COMPACT, 1, device) exceeds that size
+ * (a problem that fits only a smaller plan runs with that plan, see DES_COMPACT).  All calls share the
  * array: calls whose work overlaps on the GPU race and corrupt each other.  The first call on each
  * device looks up the array's address (cudaGetSymbolAddress); make it before any stream capture.
  * Allocates nothing. */

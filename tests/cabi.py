@@ -14,6 +14,7 @@ LIBPATH = os.path.join(ROOT, "diff_envshade_b200", "libdes_b200.so")
 DES_OK, DES_ERR_INVALID_ARGUMENT, DES_ERR_UNSUPPORTED, DES_ERR_WORKSPACE, DES_ERR_CUDA, DES_ERR_BAD_INDEX = range(6)
 DES_DIFFUSE, DES_SPECULAR, DES_CLAMP = 1, 2, 4
 DES_INPUT_ORDER = 16
+DES_COMPACT = 32
 
 vp = ctypes.c_void_p
 

@@ -296,7 +296,7 @@ def test_point_ordering_changes_no_result(des, P, layout):
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     dev = torch.cuda.current_device()
     res = {}
-    for order in (0, cabi.DES_INPUT_ORDER):
+    for order in (0, cabi.DES_INPUT_ORDER, cabi.DES_COMPACT):
         flags = cabi.DES_DIFFUSE | cabi.DES_SPECULAR | order
         wsf = L.des_shade_workspace_bytes(args.P, args.H, args.W, flags, 0, dev)
         wsb = L.des_shade_workspace_bytes(args.P, args.H, args.W, flags, 1, dev)
@@ -313,9 +313,13 @@ def test_point_ordering_changes_no_result(des, P, layout):
     both = cabi.DES_DIFFUSE | cabi.DES_SPECULAR
     assert L.des_shade_workspace_bytes(args.P, args.H, args.W, both, 1, dev) > \
         L.des_shade_workspace_bytes(args.P, args.H, args.W, both | cabi.DES_INPUT_ORDER, 1, dev)
+    assert L.des_shade_workspace_bytes(args.P, args.H, args.W, both | cabi.DES_COMPACT, 1, dev) <= \
+        L.des_shade_workspace_bytes(args.P, args.H, args.W, both | cabi.DES_INPUT_ORDER, 1, dev)
     torch.cuda.synchronize()
-    for name, a, b in zip(("shading", "diffuse_shading") + GRAD_KEYS, res[0], res[cabi.DES_INPUT_ORDER]):
-        if name == "g_env":
-            assert_close_grad(a.cpu(), b.cpu(), "ordered-vs-input:g_env")
-        else:
-            assert torch.equal(a, b), f"ordered and input order differ in {name}"
+    for other in (cabi.DES_INPUT_ORDER, cabi.DES_COMPACT):
+        for name, a, b in zip(("shading", "diffuse_shading") + GRAD_KEYS, res[0], res[other]):
+            if name == "g_env" or (other == cabi.DES_COMPACT and name.startswith("g_")):
+                # compact: the adjoint splits each point's texel sum over a different number of warps
+                assert_close_grad(a.cpu(), b.cpu(), f"plan {other}:{name}")
+            else:
+                assert torch.equal(a, b), f"default plan and plan {other} differ in {name}"
