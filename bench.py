@@ -8,7 +8,8 @@ one backward (..._backward2) per step.  Metric = points * texels / (t_fwd + t_bw
 
 Timing: W untimed warm-up steps; then K steps, each bracketed by CUDA events on the launching
 stream; a 256 MiB buffer larger than the 126 MB L2 is rewritten between timed steps (outside the
-events).  Multi-GPU (torchrun): every rank shades its own 70k points (weak scaling) and the
+events), and the normals are marked modified before every step (as an optimizer update would), so
+the only ordering reused is the one the step's own forward computed for its backward.  Multi-GPU (torchrun): every rank shades its own 70k points (weak scaling) and the
 env-map gradients are summed over ranks with one NCCL all-reduce (the path's only exchange);
 the reported time is the max over ranks.
 
@@ -230,6 +231,7 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def step():
+        torch.autograd.graph.increment_version(d.normal)
         sh, wh = des.bruteforce_specularvisibility_shader_forward2(
             d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness, d.envmap, d.light2obj_rotmat, *vis, True)
         g = des.bruteforce_specularvisibility_shader_backward2(
@@ -258,6 +260,10 @@ def main():
     launches0 = des.kernel_launches()
     for i in range(K):
         flush.fill_(float(i))
+        # a training step changes the points every step (the optimizer update): mark the normals as
+        # modified so that no step can reuse an earlier step's point ordering -- only the backward
+        # reuses the ordering its own forward computed
+        torch.autograd.graph.increment_version(d.normal)
         ev[i][0].record()
         des.set_timing_events(kf[i][0].cuda_event, kf[i][1].cuda_event)
         sh, wh = des.bruteforce_specularvisibility_shader_forward2(

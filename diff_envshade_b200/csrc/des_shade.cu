@@ -719,16 +719,22 @@ LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev, bool com
   return lp;
 }
 
+// Workspace layout: control words | texel table | ordering (when ordering) | env partials (adjoint).
+// The permutation starts at the same offset in the forward's and the adjoint's workspace of a
+// problem, so one buffer can carry a forward's ordering into the adjoint (DES_REUSE_ORDER).
+size_t sort_area_bytes(const LaunchPlan& lp) {
+  if (!lp.sort) return 0;
+  return align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256) +             // permutation
+         align_up((size_t)kSortBins * sort_row(lp) * sizeof(unsigned), 256) +  // cell counts [cell][chunk]
+         align_up((size_t)lp.ntiles * 32 * sizeof(uint16_t), 256) +            // cell of each point
+         align_up((size_t)lp.ntiles * 32 * sizeof(uint32_t), 256);             // rank of each point
+}
+
 size_t workspace_bytes(const LaunchPlan& lp, bool backward, int grid) {
   size_t off = kCtrlBytes;
   off += align_up((size_t)lp.HWpad * 32, 256);  // texel table
+  off += sort_area_bytes(lp);
   if (backward) off += align_up((size_t)std::max(grid, 1) * 3 * lp.HWpad * sizeof(double), 256);
-  if (lp.sort) {
-    off += align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256);                 // permutation
-    off += align_up((size_t)kSortBins * sort_row(lp) * sizeof(unsigned), 256);      // cell counts [cell][chunk]
-    off += align_up((size_t)lp.ntiles * 32 * sizeof(uint16_t), 256);                // cell of each point
-    off += align_up((size_t)lp.ntiles * 32 * sizeof(uint32_t), 256);                // rank of each point
-  }
   return off;
 }
 
@@ -797,10 +803,8 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   unsigned char* ws = static_cast<unsigned char*>(call.workspace);
   unsigned* ctrl = reinterpret_cast<unsigned*>(ws);
   float4* table = reinterpret_cast<float4*>(ws + kCtrlBytes);
-  double* env_partial = reinterpret_cast<double*>(ws + kCtrlBytes + align_up((size_t)lp.HWpad * 32, 256));
-  unsigned char* sort_area =
-      ws + kCtrlBytes + align_up((size_t)lp.HWpad * 32, 256) +
-      (call.backward ? align_up((size_t)std::max(grid, 1) * 3 * lp.HWpad * sizeof(double), 256) : 0);
+  unsigned char* sort_area = ws + kCtrlBytes + align_up((size_t)lp.HWpad * 32, 256);
+  double* env_partial = reinterpret_cast<double*>(sort_area + sort_area_bytes(lp));
   int32_t* perm = reinterpret_cast<int32_t*>(sort_area);
   unsigned* sort_counts =
       reinterpret_cast<unsigned*>(sort_area + align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256));
@@ -809,9 +813,11 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   uint32_t* sort_rank = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(sort_keys) +
                                                     align_up((size_t)lp.ntiles * 32 * sizeof(uint16_t), 256));
 
-  // texel table + control-word reset (+ step 1 of the ordering when ordering)
+  // texel table + control-word reset (+ step 1 of the ordering when ordering, unless the workspace
+  // already holds this problem's ordering from the previous call on it)
   const bool sort = lp.sort && a.P > 0 && (diff || spec);
-  if (sort) {
+  const bool reuse = sort && (call.flags & DES_REUSE_ORDER) != 0;
+  if (sort && !reuse) {
     des_prep_kernel<<<lp.sort_chunks, kSortThreads, 0, stream>>>(a.H, a.W, lp.HWpad, a.light2obj_rotmat, a.envmap,
                                                                  table, ctrl, a.normal, a.P, lp.sort_chunk,
                                                                  sort_row(lp), sort_counts, sort_keys, sort_rank);
@@ -878,13 +884,13 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   prm.env_partial = env_partial;
   prm.env_in_smem = lp.env_in_smem;
   prm.perm = nullptr;
-  if (sort) {
+  if (sort && !reuse) {
     des_place_kernel<<<lp.sort_chunks, kSortBins, 0, stream>>>(a.P, lp.sort_chunk, lp.sort_chunks, sort_row(lp),
                                                                sort_counts, sort_keys, sort_rank, perm);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
     count_launches(1);
-    prm.perm = perm;
   }
+  if (sort) prm.perm = perm;
 
   KernelFn k = call.backward ? pick<BwdSel>(diff, spec, vis) : pick<FwdSel>(diff, spec, vis);
   cudaEvent_t ev0 = g_timing_start.load(), ev1 = g_timing_stop.load();

@@ -13,7 +13,9 @@
 #include <c10/cuda/CUDAGuard.h>
 #include <torch/extension.h>
 
+#include <algorithm>
 #include <cstdlib>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -120,12 +122,6 @@ VisArgs vis_checks(const Common& c, const Tensor& faces, const Tensor& tri, cons
   return v;
 }
 
-Tensor workspace(const Tensor& like, const Common& c, unsigned flags, bool backward) {
-  const size_t bytes = des_shade_workspace_bytes(c.P, c.H, c.W, flags, backward ? 1 : 0, like.get_device());
-  TORCH_CHECK(bytes > 0, "diff_envshade_b200: could not size the workspace");
-  return torch::empty({(int64_t)bytes}, like.options().dtype(torch::kUInt8));
-}
-
 void finish(int st, Tensor& ws, cudaStream_t stream) {
   raise_status(st);
   if (check_indices_enabled()) {
@@ -135,6 +131,125 @@ void finish(int st, Tensor& ws, cudaStream_t stream) {
     raise_status(status);
   }
 }
+
+des_stream_t cur_stream_h() { return reinterpret_cast<des_stream_t>(at::cuda::getCurrentCUDAStream().stream()); }
+
+// One shading workspace per device, reused by consecutive calls on the same stream (sized for both
+// the forward and the adjoint of a problem).  When a call passes the same points as the previous
+// successful call on it -- the same normal tensor storage, offset, point count and version, and
+// the same map size -- the workspace still holds their normal-direction ordering and the call skips
+// recomputing it (DES_REUSE_ORDER): the adjoint after its forward, the usual pattern.  A call on
+// another stream gets a fresh buffer (never one that another stream may still be using).  The entry
+// holds a reference to the normals' storage, so that storage cannot be freed and its address reused
+// by other points while the entry exists (the most recent normals stay allocated until the next call).
+struct WsEntry {
+  Tensor ws;
+  cudaStream_t stream = nullptr;
+  c10::Storage storage;
+  int64_t offset = -1, P = -1;
+  uint32_t version = 0;
+  int H = 0, W = 0;
+  bool holds_order = false;
+};
+std::mutex g_ws_mu;
+WsEntry g_ws[64];
+
+struct WsLease {
+  Tensor ws;
+  unsigned extra = 0;  // DES_REUSE_ORDER when the workspace holds these points' ordering
+  int dev = 0;
+};
+
+WsLease lease_workspace(const Tensor& normal, const Common& c, unsigned flags) {
+  WsLease L;
+  L.dev = normal.get_device();
+  TORCH_CHECK(L.dev >= 0 && L.dev < 64, "diff_envshade_b200: device index out of range");
+  const size_t need = std::max(des_shade_workspace_bytes(c.P, c.H, c.W, flags, 0, L.dev),
+                               des_shade_workspace_bytes(c.P, c.H, c.W, flags, 1, L.dev));
+  TORCH_CHECK(need > 0, "diff_envshade_b200: could not size the workspace");
+  const cudaStream_t stream = at::cuda::getCurrentCUDAStream().stream();
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  WsEntry& e = g_ws[L.dev];
+  if (!e.ws.defined() || e.stream != stream || (size_t)e.ws.numel() < need) {
+    e = WsEntry{};
+    e.ws = torch::empty({(int64_t)need}, normal.options().dtype(torch::kUInt8));
+    e.stream = stream;
+  }
+  const bool same = e.holds_order && e.storage.unsafeGetStorageImpl() == normal.storage().unsafeGetStorageImpl() &&
+                    e.offset == normal.storage_offset() && e.P == c.P && e.version == normal._version() &&
+                    e.H == c.H && e.W == c.W;
+  L.ws = e.ws;
+  L.extra = same ? DES_REUSE_ORDER : 0u;
+  e.holds_order = false;  // until this call has succeeded
+  return L;
+}
+
+// After a successful call: the workspace now holds the ordering of these points.
+void workspace_done(const WsLease& L, const Tensor& normal, const Common& c) {
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  WsEntry& e = g_ws[L.dev];
+  if (!e.ws.defined() || !e.ws.is_same(L.ws)) return;
+  e.storage = normal.storage();
+  e.offset = normal.storage_offset();
+  e.P = c.P;
+  e.version = normal._version();
+  e.H = c.H;
+  e.W = c.W;
+  e.holds_order = true;
+}
+
+des_shade_args make_args(const Common& c, const Tensor& normal, const Tensor* view, const Tensor& albedo,
+                         const Tensor* spec, const Tensor* rough, const Tensor& envmap, const Tensor& R) {
+  des_shade_args a{};
+  a.P = c.P;
+  a.H = c.H;
+  a.W = c.W;
+  a.C = (int32_t)c.C;
+  a.normal = normal.data_ptr<float>();
+  a.view_dir = view ? view->data_ptr<float>() : nullptr;
+  a.albedo = albedo.data_ptr<float>();
+  a.specular_albedo = spec ? spec->data_ptr<float>() : nullptr;
+  a.roughness = rough ? rough->data_ptr<float>() : nullptr;
+  a.envmap = envmap.data_ptr<float>();
+  a.light2obj_rotmat = R.data_ptr<float>();
+  return a;
+}
+
+void add_visibility(des_shade_args& a, const VisArgs& v, const Tensor& faces, const Tensor& tri, const Tensor& bary,
+                    const Tensor& vis) {
+  a.N_face = v.N_face;
+  a.N_vertex = v.N_vertex;
+  a.N_slot = v.N_slot;
+  a.face_vertex_list = faces.data_ptr<int32_t>();
+  a.nearest_triangle_id = tri.data_ptr<int64_t>();
+  a.barycentric_coord = bary.data_ptr<float>();
+  a.visibility = reinterpret_cast<const uint32_t*>(vis.data_ptr<int32_t>());
+}
+
+// The forward / adjoint of one operator through the shared workspace.
+int run_forward(const des_shade_args& a, const Tensor& normal, const Common& c, unsigned flags, Tensor& shading,
+                Tensor* white) {
+  WsLease L = lease_workspace(normal, c, flags);
+  const int st = des_shade_forward(&a, flags | L.extra, shading.data_ptr<float>(),
+                                   white ? white->data_ptr<float>() : nullptr, L.ws.data_ptr(), (size_t)L.ws.numel(),
+                                   cur_stream_h());
+  if (st == DES_OK) workspace_done(L, normal, c);
+  finish(st, L.ws, at::cuda::getCurrentCUDAStream().stream());
+  return st;
+}
+
+int run_backward(const des_shade_args& a, const Tensor& normal, const Common& c, unsigned flags, const Tensor& gsh,
+                 const Tensor* gwh, Tensor& gn, Tensor* gv, Tensor& ga, Tensor* gs, Tensor* gr, Tensor& genv) {
+  WsLease L = lease_workspace(normal, c, flags);
+  const int st = des_shade_backward(&a, flags | L.extra, gsh.data_ptr<float>(), gwh ? gwh->data_ptr<float>() : nullptr,
+                                    gn.data_ptr<float>(), gv ? gv->data_ptr<float>() : nullptr, ga.data_ptr<float>(),
+                                    gs ? gs->data_ptr<float>() : nullptr, gr ? gr->data_ptr<float>() : nullptr,
+                                    genv.data_ptr<float>(), L.ws.data_ptr(), (size_t)L.ws.numel(), cur_stream_h());
+  if (st == DES_OK) workspace_done(L, normal, c);
+  finish(st, L.ws, at::cuda::getCurrentCUDAStream().stream());
+  return st;
+}
+
 
 const float* fptr(const Tensor& t) { return t.data_ptr<float>(); }
 float* fptr_mut(Tensor& t) { return t.data_ptr<float>(); }
@@ -150,12 +265,8 @@ Tensor bruteforce_diffuse_shader_forward(const Tensor& normal, const Tensor& alb
   const at::cuda::OptionalCUDAGuard guard(device_of(normal));
   auto opt = normal.options().requires_grad(false);
   Tensor shading = torch::empty({c.P, c.C}, opt);
-  Tensor ws = workspace(normal, c, DES_DIFFUSE, false);
-  auto stream = at::cuda::getCurrentCUDAStream().stream();
-  int st = des_bruteforce_diffuse_shader_forward(c.P, c.H, c.W, (int)c.C, fptr(normal), fptr(albedo), fptr(envmap),
-                                                 fptr(R), fptr_mut(shading), ws.data_ptr(), (size_t)ws.numel(),
-                                                 cur_stream());
-  finish(st, ws, stream);
+  const des_shade_args a = make_args(c, normal, nullptr, albedo, nullptr, nullptr, envmap, R);
+  run_forward(a, normal, c, DES_DIFFUSE, shading, nullptr);
   return shading;
 }
 
@@ -169,13 +280,8 @@ std::vector<Tensor> bruteforce_diffuse_shader_backward(const Tensor& grad_shadin
   Tensor g_albedo = torch::empty({c.P, c.C}, opt);
   Tensor g_normal = torch::empty({c.P, 3}, opt);
   Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
-  Tensor ws = workspace(normal, c, DES_DIFFUSE, true);
-  auto stream = at::cuda::getCurrentCUDAStream().stream();
-  int st = des_bruteforce_diffuse_shader_backward(c.P, c.H, c.W, (int)c.C, fptr(grad_shading), fptr(normal),
-                                                  fptr(albedo), fptr(envmap), fptr(R), fptr_mut(g_normal),
-                                                  fptr_mut(g_albedo), fptr_mut(g_env), ws.data_ptr(),
-                                                  (size_t)ws.numel(), cur_stream());
-  finish(st, ws, stream);
+  const des_shade_args a = make_args(c, normal, nullptr, albedo, nullptr, nullptr, envmap, R);
+  run_backward(a, normal, c, DES_DIFFUSE, grad_shading, nullptr, g_normal, nullptr, g_albedo, nullptr, nullptr, g_env);
   return {g_normal, g_albedo, g_env};
 }
 
@@ -188,13 +294,8 @@ Tensor specular_forward_impl(const Tensor& normal, const Tensor& view, const Ten
   auto opt = normal.options().requires_grad(false);
   Tensor shading = torch::empty({c.P, c.C}, opt);
   unsigned f = (enable_diffuse ? DES_DIFFUSE : 0u) | (enable_specular ? DES_SPECULAR : 0u) | (clamp ? DES_CLAMP : 0u);
-  Tensor ws = workspace(normal, c, f, false);
-  auto stream = at::cuda::getCurrentCUDAStream().stream();
-  int st = des_bruteforce_specular_shader_forward(c.P, c.H, c.W, (int)c.C, fptr(normal), fptr(view), fptr(albedo),
-                                                  fptr(spec), fptr(rough), fptr(envmap), fptr(R), enable_diffuse,
-                                                  enable_specular, clamp, fptr_mut(shading), ws.data_ptr(),
-                                                  (size_t)ws.numel(), cur_stream());
-  finish(st, ws, stream);
+  const des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
+  run_forward(a, normal, c, f, shading, nullptr);
   return shading;
 }
 
@@ -215,14 +316,8 @@ std::vector<Tensor> specular_backward_impl(const Tensor& grad_shading, const Ten
   Tensor g_rough = torch::empty({c.P, 1}, opt);
   Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
   unsigned f = (enable_diffuse ? DES_DIFFUSE : 0u) | (enable_specular ? DES_SPECULAR : 0u) | (clamp ? DES_CLAMP : 0u);
-  Tensor ws = workspace(normal, c, f, true);
-  auto stream = at::cuda::getCurrentCUDAStream().stream();
-  int st = des_bruteforce_specular_shader_backward(
-      c.P, c.H, c.W, (int)c.C, fptr(grad_shading), fptr(normal), fptr(view), fptr(albedo), fptr(spec), fptr(rough),
-      fptr(envmap), fptr(R), enable_diffuse, enable_specular, clamp, fptr_mut(g_normal), fptr_mut(g_view),
-      fptr_mut(g_albedo), fptr_mut(g_spec), fptr_mut(g_rough), fptr_mut(g_env), ws.data_ptr(), (size_t)ws.numel(),
-      cur_stream());
-  finish(st, ws, stream);
+  const des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
+  run_backward(a, normal, c, f, grad_shading, nullptr, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
   return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
 }
 
@@ -264,13 +359,8 @@ std::vector<Tensor> bruteforce_specular_shader_forward2(const Tensor& normal, co
   Tensor shading = torch::empty({c.P, c.C}, opt);
   Tensor white = torch::empty({c.P, c.C}, opt);
   unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
-  Tensor ws = workspace(normal, c, f, false);
-  auto stream = at::cuda::getCurrentCUDAStream().stream();
-  int st = des_bruteforce_specular_shader_forward2(c.P, c.H, c.W, (int)c.C, fptr(normal), fptr(view), fptr(albedo),
-                                                   fptr(spec), fptr(rough), fptr(envmap), fptr(R), enable_specular,
-                                                   fptr_mut(shading), fptr_mut(white), ws.data_ptr(),
-                                                   (size_t)ws.numel(), cur_stream());
-  finish(st, ws, stream);
+  const des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
+  run_forward(a, normal, c, f, shading, &white);
   return {shading, white};
 }
 
@@ -294,14 +384,8 @@ std::vector<Tensor> bruteforce_specular_shader_backward2(const Tensor& grad_shad
   Tensor g_rough = torch::empty({c.P, 1}, opt);
   Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
   unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
-  Tensor ws = workspace(normal, c, f, true);
-  auto stream = at::cuda::getCurrentCUDAStream().stream();
-  int st = des_bruteforce_specular_shader_backward2(
-      c.P, c.H, c.W, (int)c.C, fptr(grad_shading), fptr(grad_white), fptr(normal), fptr(view), fptr(albedo),
-      fptr(spec), fptr(rough), fptr(envmap), fptr(R), enable_specular, fptr_mut(g_normal), fptr_mut(g_view),
-      fptr_mut(g_albedo), fptr_mut(g_spec), fptr_mut(g_rough), fptr_mut(g_env), ws.data_ptr(), (size_t)ws.numel(),
-      cur_stream());
-  finish(st, ws, stream);
+  const des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
+  run_backward(a, normal, c, f, grad_shading, &grad_white, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
   return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
 }
 
@@ -317,14 +401,9 @@ std::vector<Tensor> bruteforce_specularvisibility_shader_forward2(
   Tensor shading = torch::empty({c.P, c.C}, opt);
   Tensor white = torch::empty({c.P, c.C}, opt);
   unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
-  Tensor ws = workspace(normal, c, f, false);
-  auto stream = at::cuda::getCurrentCUDAStream().stream();
-  int st = des_bruteforce_specularvisibility_shader_forward2(
-      c.P, c.H, c.W, (int)c.C, v.N_face, v.N_vertex, v.N_slot, fptr(normal), fptr(view), fptr(albedo), fptr(spec),
-      fptr(rough), fptr(envmap), fptr(R), faces.data_ptr<int32_t>(), tri.data_ptr<int64_t>(), fptr(bary),
-      vis.data_ptr<int32_t>(), enable_specular, fptr_mut(shading), fptr_mut(white), ws.data_ptr(),
-      (size_t)ws.numel(), cur_stream());
-  finish(st, ws, stream);
+  des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
+  add_visibility(a, v, faces, tri, bary, vis);
+  run_forward(a, normal, c, f, shading, &white);
   return {shading, white};
 }
 
@@ -348,15 +427,9 @@ std::vector<Tensor> bruteforce_specularvisibility_shader_backward2(
   Tensor g_rough = torch::empty({c.P, 1}, opt);
   Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
   unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
-  Tensor ws = workspace(normal, c, f, true);
-  auto stream = at::cuda::getCurrentCUDAStream().stream();
-  int st = des_bruteforce_specularvisibility_shader_backward2(
-      c.P, c.H, c.W, (int)c.C, v.N_face, v.N_vertex, v.N_slot, fptr(grad_shading), fptr(grad_white), fptr(normal),
-      fptr(view), fptr(albedo), fptr(spec), fptr(rough), fptr(envmap), fptr(R), faces.data_ptr<int32_t>(),
-      tri.data_ptr<int64_t>(), fptr(bary), vis.data_ptr<int32_t>(), enable_specular, fptr_mut(g_normal),
-      fptr_mut(g_view), fptr_mut(g_albedo), fptr_mut(g_spec), fptr_mut(g_rough), fptr_mut(g_env), ws.data_ptr(),
-      (size_t)ws.numel(), cur_stream());
-  finish(st, ws, stream);
+  des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
+  add_visibility(a, v, faces, tri, bary, vis);
+  run_backward(a, normal, c, f, grad_shading, &grad_white, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
   return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
 }
 

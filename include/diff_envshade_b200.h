@@ -56,6 +56,15 @@ typedef enum des_status {
  * texel sum is split over a different number of warps).  A workspace too small for the default
  * plan also falls back to input order, then to this plan. */
 #define DES_COMPACT 32u
+/* des_shade_*: the workspace already holds the point ordering of these same normals (same P, H, W)
+ * from the previous call made with it -- typically the forward of the adjoint that follows -- so the
+ * ordering kernels are skipped.  Only the caller can know this: the workspace must not have been
+ * used for anything else in between (a damaged permutation loses points; entries out of range
+ * are skipped and reported as DES_ERR_BAD_INDEX by des_workspace_status).  If only the normals'
+ * values changed, the stale ordering is still a valid permutation: per-point outputs are the same
+ * bit for bit and the env-map gradient differs only in FP64 summation order.  Ignored for calls
+ * that do not order their points. */
+#define DES_REUSE_ORDER 64u
 
 /* All inputs of one shading call.  The visibility block is ignored when visibility == NULL. */
 typedef struct des_shade_args {

@@ -15,6 +15,7 @@ DES_OK, DES_ERR_INVALID_ARGUMENT, DES_ERR_UNSUPPORTED, DES_ERR_WORKSPACE, DES_ER
 DES_DIFFUSE, DES_SPECULAR, DES_CLAMP = 1, 2, 4
 DES_INPUT_ORDER = 16
 DES_COMPACT = 32
+DES_REUSE_ORDER = 64
 
 vp = ctypes.c_void_p
 

@@ -323,3 +323,61 @@ def test_point_ordering_changes_no_result(des, P, layout):
                 assert_close_grad(a.cpu(), b.cpu(), f"plan {other}:{name}")
             else:
                 assert torch.equal(a, b), f"default plan and plan {other} differ in {name}"
+
+
+def test_backward_reuses_its_forwards_ordering(des):
+    """The torch ops keep one workspace per device: a backward that follows its forward on the same
+    normals skips the two ordering kernels (3 launches instead of 4); modifying the normals (their
+    version counter) makes the next call order the points again."""
+    from diff_envshade_b200 import workloads as wl
+    d = _dev(wl.make_inputs(70000, 16, 32, seed=91, vis_p=0.7, rotation=True))
+    base = (d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness, d.envmap, d.light2obj_rotmat)
+    vis = (d.face_vertex_list, d.nearest_triangle_id, d.barycentric_coord, d.visibility)
+    gs, gw = d.grad_shading, d.grad_diffuse_shading
+    n0 = des.kernel_launches()
+    des.bruteforce_specularvisibility_shader_forward2(*base, *vis, True)
+    n1 = des.kernel_launches()
+    g = des.bruteforce_specularvisibility_shader_backward2(gs, gw, *base, *vis, True)
+    n2 = des.kernel_launches()
+    assert n1 - n0 == 3 and n2 - n1 == 3, (n1 - n0, n2 - n1)  # fwd: prep, place, shade; bwd: table, shade, reduce
+    torch.autograd.graph.increment_version(d.normal)
+    g2 = des.bruteforce_specularvisibility_shader_backward2(gs, gw, *base, *vis, True)
+    n3 = des.kernel_launches()
+    assert n3 - n2 == 4  # ordered again: prep, place, shade, reduce
+    for a, b in zip(g[:5], g2[:5]):
+        assert torch.equal(a, b)
+    assert_close_grad(g[5].cpu(), g2[5].cpu(), "reuse:g_env")
+
+
+def test_stale_ordering_changes_no_result(des):
+    """DES_REUSE_ORDER with an ordering computed for other normals (same P): per-point outputs are
+    bit-identical to a fresh call, the env-map gradient within the gradient bound."""
+    from diff_envshade_b200 import workloads as wl
+    P = 50000
+    A = _dev(wl.make_inputs(P, 16, 32, seed=92, vis_p=0.7))
+    B = _dev(wl.make_inputs(P, 16, 32, seed=93, vis_p=0.7))
+    L = cabi.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    flags = cabi.DES_DIFFUSE | cabi.DES_SPECULAR
+    dev = torch.cuda.current_device()
+    argsA, argsB = cabi.make_args(A), cabi.make_args(B)
+    wsb = max(L.des_shade_workspace_bytes(P, 16, 32, flags, k, dev) for k in (0, 1))
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    shA = torch.empty(P, 3, device="cuda")
+    assert L.des_shade_forward(ctypes.byref(argsA), flags, cabi.ptr(shA), None, cabi.ptr(ws), wsb, stream) == 0
+
+    def backward(extra, wsx):
+        outs = [torch.empty(P, 3, device="cuda") for _ in range(4)] + [torch.empty(P, 1, device="cuda"),
+                                                                        torch.empty(3, 16, 32, device="cuda")]
+        st = L.des_shade_backward(ctypes.byref(argsB), flags | extra, cabi.ptr(B.grad_shading),
+                                  cabi.ptr(B.grad_diffuse_shading), *[cabi.ptr(o) for o in outs], cabi.ptr(wsx), wsb,
+                                  stream)
+        assert st == 0
+        return outs
+
+    stale = backward(cabi.DES_REUSE_ORDER, ws)  # ordering of A's normals applied to B
+    fresh = backward(0, torch.empty(wsb, dtype=torch.uint8, device="cuda"))
+    torch.cuda.synchronize()
+    for a, b in zip(stale[:5], fresh[:5]):
+        assert torch.equal(a, b)
+    assert_close_grad(stale[5].cpu(), fresh[5].cpu(), "stale:g_env")
