@@ -343,7 +343,12 @@ def main():
 
     # ---- roofline of the dominant kernel (fused adjoint) and of the forward kernel
     peaks = measured_peaks()
-    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    if "sm_max_mhz" in peaks:
+        sm_max, clock_src = float(peaks["sm_max_mhz"]), "sm_max_mhz of MEASURED_PEAKS.json"
+    elif clocks and clocks.get("sm_max_mhz"):
+        sm_max, clock_src = float(clocks["sm_max_mhz"]), "NVML max SM clock; MEASURED_PEAKS.json absent"
+    else:
+        sm_max, clock_src = 1965.0, "nominal B200 max SM clock; no measured clock"
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     peak_tinst = sms * FP32_LANES_PER_SM * sm_max * 1e6 / 1e12
     bwd_avg = float(np.mean(bwd_ms)) * 1e-3
@@ -355,7 +360,7 @@ def main():
         "achieved": ach_bwd, "peak": peak_tinst, "unit": "T FP32-pipe instr/s", "frac": ach_bwd / peak_tinst,
         "traffic": committed_traffic(),
         "peak_source": f"derived: {sms} SMs x {FP32_LANES_PER_SM} FP32 lanes x {sm_max:.0f} MHz "
-                       "(sm_max_mhz of MEASURED_PEAKS.json; no measured FP32 peak exists)",
+                       f"({clock_src}; no measured FP32 peak exists)",
         "work": f"{INSTR_BWD_VIS} FP32-pipe instr per point*texel pair x {P}x{HW} pairs per launch",
         "kernel_ms": bwd_avg * 1e3,
         "forward": {"kernel_ms": fwd_avg * 1e3, "achieved": ach_fwd, "frac": ach_fwd / peak_tinst,
