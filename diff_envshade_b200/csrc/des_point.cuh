@@ -310,12 +310,17 @@ struct BwdOutputs {
   float *g_normal, *g_view, *g_albedo, *g_spec, *g_rough;
 };
 
-// Finishes one point from its reduced adjoint sums (BwdAcc order): applies the Schlick-Smith view
-// factor (bruteforce_shader.cu:194-200) and the roughness chain rule (2501-2502) and stores the
-// point's gradients.  r = roughness, g_shading3 = the point's incoming shading gradient.
+// One point's gradients from its reduced adjoint sums (BwdAcc order): applies the Schlick-Smith
+// view factor (bruteforce_shader.cu:194-200) and the roughness chain rule (2501-2502).
+// r = roughness, (g0, g1, g2) = the point's incoming shading gradient.
+struct BwdGrads {
+  float n[3], v[3], a[3], s[3], rough;
+};
+
 template <bool DIFF, bool SPEC>
-__device__ __forceinline__ void finish_bwd_point(const float (&sums)[15], const PointGeom& g, const SpecConst& sc,
-                                                 float r, const float* g_shading3, int64_t pid, const BwdOutputs& o) {
+__device__ __forceinline__ BwdGrads bwd_point_grads(const float (&sums)[15], const PointGeom& g, const SpecConst& sc,
+                                                    float r, float g0, float g1, float g2) {
+  BwdGrads q;
   float n_x = sums[6], n_y = sums[7], n_z = sums[8];
   float v_x = sums[9], v_y = sums[10], v_z = sums[11];
   float g_rough = 0.f;
@@ -335,26 +340,54 @@ __device__ __forceinline__ void finish_bwd_point(const float (&sums)[15], const 
     g_rough = sums[13] * 4.f * r * r * r;
     g_rough += gk * (1.f + r) / 4.f;
   }
-  o.g_normal[3 * pid] = n_x;
-  o.g_normal[3 * pid + 1] = n_y;
-  o.g_normal[3 * pid + 2] = n_z;
-  const float g0 = g_shading3[0], g1 = g_shading3[1], g2 = g_shading3[2];
-  if (o.g_albedo != nullptr) {
-    o.g_albedo[3 * pid] = DIFF ? g0 * sums[0] : 0.f;
-    o.g_albedo[3 * pid + 1] = DIFF ? g1 * sums[1] : 0.f;
-    o.g_albedo[3 * pid + 2] = DIFF ? g2 * sums[2] : 0.f;
+  q.n[0] = n_x;
+  q.n[1] = n_y;
+  q.n[2] = n_z;
+  q.a[0] = DIFF ? g0 * sums[0] : 0.f;
+  q.a[1] = DIFF ? g1 * sums[1] : 0.f;
+  q.a[2] = DIFF ? g2 * sums[2] : 0.f;
+  q.s[0] = SPEC ? g0 * sums[3] : 0.f;
+  q.s[1] = SPEC ? g1 * sums[4] : 0.f;
+  q.s[2] = SPEC ? g2 * sums[5] : 0.f;
+  q.v[0] = SPEC ? v_x : 0.f;
+  q.v[1] = SPEC ? v_y : 0.f;
+  q.v[2] = SPEC ? v_z : 0.f;
+  q.rough = g_rough;
+  return q;
+}
+
+// Finishes one point: its gradients (bwd_point_grads) stored at index pid.  g_shading3 = the
+// point's incoming shading gradient.
+template <bool DIFF, bool SPEC>
+__device__ __forceinline__ void finish_bwd_point(const float (&sums)[15], const PointGeom& g, const SpecConst& sc,
+                                                 float r, const float* g_shading3, int64_t pid, const BwdOutputs& o) {
+  const BwdGrads q = bwd_point_grads<DIFF, SPEC>(sums, g, sc, r, g_shading3[0], g_shading3[1], g_shading3[2]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) o.g_normal[3 * pid + c] = q.n[c];
+  if (o.g_albedo != nullptr)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.g_albedo[3 * pid + c] = q.a[c];
+  if (o.g_spec != nullptr)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.g_spec[3 * pid + c] = q.s[c];
+  if (o.g_view != nullptr)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.g_view[3 * pid + c] = q.v[c];
+  if (o.g_rough != nullptr) o.g_rough[pid] = q.rough;
+}
+
+// Stores the 3-vectors of a tile's 32 consecutive points (lane = point, first point `first`, P
+// points in all) as whole 128-byte rows: round k writes floats 32k .. 32k+31 of the tile's 96, each
+// lane fetching its value from the owning lane by shuffle.  All 32 lanes take part.
+__device__ __forceinline__ void store_rows3(float* dst, int64_t first, int64_t P, float x, float y, float z,
+                                            int lane) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int f = 32 * k + lane, p = f / 3, c = f - 3 * p;
+    const float a = __shfl_sync(0xffffffffu, x, p), b = __shfl_sync(0xffffffffu, y, p),
+                d = __shfl_sync(0xffffffffu, z, p);
+    if (first + p < P) dst[3 * first + f] = c == 0 ? a : (c == 1 ? b : d);
   }
-  if (o.g_spec != nullptr) {
-    o.g_spec[3 * pid] = SPEC ? g0 * sums[3] : 0.f;
-    o.g_spec[3 * pid + 1] = SPEC ? g1 * sums[4] : 0.f;
-    o.g_spec[3 * pid + 2] = SPEC ? g2 * sums[5] : 0.f;
-  }
-  if (o.g_view != nullptr) {
-    o.g_view[3 * pid] = SPEC ? v_x : 0.f;
-    o.g_view[3 * pid + 1] = SPEC ? v_y : 0.f;
-    o.g_view[3 * pid + 2] = SPEC ? v_z : 0.f;
-  }
-  if (o.g_rough != nullptr) o.g_rough[pid] = g_rough;
 }
 
 }  // namespace des

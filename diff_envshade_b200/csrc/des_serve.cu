@@ -4,20 +4,25 @@
 // scheduler thread
 //   * admits them in arrival order while a device arena of fixed size (the HBM budget) has room,
 //     skipping over requests that do not fit yet, and uploads their point data through a copy lane
-//     that sends the least remaining work first, in slices (downloads use a second lane);
+//     that sends the least remaining work first, in slices (downloads use a second lane); requests
+//     shaded in input order whose buffers the device can reach (its own memory, pinned host
+//     memory) skip the copies: the batch kernel reads their inputs and stores their outputs in
+//     place;
 //   * keeps env maps (their texel tables) and meshes (faces + visibility words) resident, shared by
 //     reference between requests;
 //   * every tick packs 32-point tiles of the admitted requests into a work list, smallest
 //     remaining work first, up to a time budget, into a work list in mapped pinned memory and
 //     launches it as a CUDA graph (one persistent batch kernel) on its own stream, with up to
-//     ticks_in_flight ticks queued so that consecutive ticks overlap;
+//     ticks_in_flight ticks queued so that consecutive ticks overlap, plus an express tick on a
+//     high-priority stream for short requests that become ready while the normal ticks are queued;
 //   * when every tile of a request has finished, copies its outputs back and frees its memory.
 // Work of different requests therefore shares each launch and each SM; a request that arrives
 // while others run joins the next tick.
 //
-// Requests of at least 16384 points are ordered by normal direction after their upload (the plain
-// path's ordering kernels, on a stream of their own), and the batch kernel skips texels below the
-// horizon of a warp's 32 points, as des_fwd_kernel / des_bwd_kernel do.
+// Requests of at least order_min_points points (off by default) are ordered by normal direction
+// after their upload (the plain path's ordering kernels, on a stream of their own); the batch
+// kernel skips texels below the horizon of a warp's 32 points, as des_fwd_kernel / des_bwd_kernel
+// do, in either order.
 // The batch kernel evaluates exactly the per-pair arithmetic of des_fwd_kernel / des_bwd_kernel
 // (shared helpers in des_point.cuh); per-point outputs are bit-identical to a solo call of the
 // batch path, and the env-map gradient is summed per request in FP64 (global FP64 atomics, then a
@@ -52,8 +57,23 @@ constexpr int kNW = 8;               // warps per CTA
 constexpr int kMaxHWpad = 2048;      // texel table kept in shared memory per CTA
 constexpr int kMaxSlots = 8192;      // concurrently admitted requests
 constexpr int kTickItems = 4096;     // work items per tick (upper bound; the whole list is uploaded)
-constexpr int kNTicks = 4;           // tick buffers (up to this many ticks in flight)
+constexpr int kNTicks = 4;           // normal tick buffers (up to this many ticks in flight)
+constexpr int kNExpress = 2;         // express tick buffers (after the normal ones), highest priority
+constexpr double kExpressTicks = 6;  // express ticks take requests with at most this many ticks of work
 constexpr int kCopyEvents = 64;                    // completion events per copy lane
+// Default ordering threshold of the server (requests of at least this many points are ordered by
+// normal direction): none.  An ordered request must be uploaded (the ordering kernels and the
+// permuted tiles read device memory), and on a busy host link those uploads slow the in-place
+// reads of every other request; the ordering kernels also wait for SMs behind the queued ticks.
+// Measured on the mixed serving workload, shading everything in input order and in place gives
+// the 50k-100k-point requests the lowest tail latency, at about a sixth less throughput than
+// ordering the requests of 128k points and more.
+constexpr int64_t kServeOrderMinP = INT64_MAX;
+// Throughput of the batch kernel on a 148-SM B200 in pair units per microsecond (a forward pair is
+// one unit, an adjoint pair two), measured on mixed workloads; it converts tick_us into work.  A
+// fixed figure: an estimate taken from the ticks themselves feeds back on itself (under-filled
+// ticks leave SMs idle, which lowers the estimate, which shrinks the ticks).
+constexpr double kBatchPairsPerUs = 3.5e5;
 
 // Device-side request descriptor (member names shared with ShadeParams for the point loaders).
 struct ReqDesc {
@@ -83,20 +103,15 @@ struct ReqDesc {
   float* g_rough;
   float* g_env;
   const int32_t* perm;       // tile slot -> point (normal-direction order), or null for input order
-  double* env_acc;           // [3][HWpad], zeroed at admission
-  unsigned* bwd_tiles_left;  // adjoint tiles not yet finished
+  double* env_acc;           // [3][HWpad], zero when the request starts (zeroed again by its last tile)
+  unsigned bwd_target;       // the slot's adjoint-tile counter after the request's last adjoint tile
+  unsigned pad_[3];
   unsigned* ctrl;            // [kCtrlError] = error word
 };
+static_assert(sizeof(ReqDesc) % 16 == 0, "descriptors are staged in 16-byte words");
 
 struct WorkItem {
   int32_t req, tile, kind, pad;  // kind 0 = forward tile, 1 = adjoint tile
-};
-
-// Pinned host staging of one slot's uploads (stays valid while the slot's request is admitted).
-struct SlotStage {
-  ReqDesc desc;
-  unsigned tiles_left;
-  unsigned pad[3];
 };
 
 // One tick's work, written by the scheduler into pinned host memory that the GPU reads directly
@@ -129,6 +144,16 @@ __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
   const PointGeom g = load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
   SpecConst sc;
   if (SPEC) sc = spec_const(valid ? r.rough[pid] : 0.f, g);
+  // the epilogue's albedos, fetched with the point (one round trip less for points read in place
+  // from host memory)
+  float alb[3] = {0.f, 0.f, 0.f}, spa[3] = {0.f, 0.f, 0.f};
+  if (warp == 0 && valid) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (DIFF) alb[c] = r.albedo[3 * pid + c];
+      if (SPEC) spa[c] = r.spec_alb[3 * pid + c];
+    }
+  }
   float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   const int nsl = r.HWpad >> 5;
   const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
@@ -169,18 +194,28 @@ __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
 #pragma unroll
   for (int q = 0; q < 6; ++q) red[q * 32] = acc[q];
   __syncthreads();
-  if (warp == 0 && valid) {
+  if (warp == 0) {
     float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int w = 0; w < kNW; ++w)
 #pragma unroll
       for (int q = 0; q < 6; ++q) s[q] += s_red[w * 6 * 32 + q * 32 + lane];
+    float out[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      float out = 0.f;
-      if (DIFF) out = r.albedo[3 * pid + c] * s[c];
-      if (SPEC) out = fmaf(r.spec_alb[3 * pid + c], s[3 + c], out);
-      r.shading[3 * pid + c] = out;
-      if (r.white != nullptr) r.white[3 * pid + c] = s[c];
+      out[c] = 0.f;
+      if (DIFF) out[c] = alb[c] * s[c];
+      if (SPEC) out[c] = fmaf(spa[c], s[3 + c], out[c]);
+    }
+    if (r.perm == nullptr) {  // consecutive points: whole-row stores (outputs may be in host memory)
+      const int64_t first = (int64_t)tile * 32;
+      store_rows3(r.shading, first, r.P, out[0], out[1], out[2], lane);
+      if (r.white != nullptr) store_rows3(r.white, first, r.P, s[0], s[1], s[2], lane);
+    } else if (valid) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        r.shading[3 * pid + c] = out[c];
+        if (r.white != nullptr) r.white[3 * pid + c] = s[c];
+      }
     }
   }
 }
@@ -272,15 +307,28 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
 #pragma unroll
   for (int q = 0; q < NACC; ++q) red[q * 32] = av[q];
   __syncthreads();
-  if (warp == 0 && valid) {
+  if (warp == 0) {
     float sums[NACC];
 #pragma unroll
     for (int q = 0; q < NACC; ++q) sums[q] = 0.f;
     for (int w = 0; w < kNW; ++w)
 #pragma unroll
       for (int q = 0; q < NACC; ++q) sums[q] += s_red[w * NACC * 32 + q * 32 + lane];
-    const BwdOutputs o{r.g_normal, r.g_view, r.g_albedo, r.g_spec, r.g_rough};
-    finish_bwd_point<DIFF, SPEC>(sums, g, sc, SPEC ? r.rough[pid] : 0.f, r.g_shading + 3 * pid, pid, o);
+    if (r.perm == nullptr) {  // consecutive points: whole-row stores (outputs may be in host memory)
+      const float rough = (SPEC && valid) ? r.rough[pid] : 0.f;
+      const float g0 = valid ? r.g_shading[3 * pid] : 0.f, g1 = valid ? r.g_shading[3 * pid + 1] : 0.f,
+                  g2 = valid ? r.g_shading[3 * pid + 2] : 0.f;
+      const BwdGrads q = bwd_point_grads<DIFF, SPEC>(sums, g, sc, rough, g0, g1, g2);
+      const int64_t first = (int64_t)tile * 32;
+      store_rows3(r.g_normal, first, r.P, q.n[0], q.n[1], q.n[2], lane);
+      if (r.g_albedo != nullptr) store_rows3(r.g_albedo, first, r.P, q.a[0], q.a[1], q.a[2], lane);
+      if (r.g_spec != nullptr) store_rows3(r.g_spec, first, r.P, q.s[0], q.s[1], q.s[2], lane);
+      if (r.g_view != nullptr) store_rows3(r.g_view, first, r.P, q.v[0], q.v[1], q.v[2], lane);
+      if (r.g_rough != nullptr && valid) r.g_rough[pid] = q.rough;
+    } else if (valid) {
+      const BwdOutputs o{r.g_normal, r.g_view, r.g_albedo, r.g_spec, r.g_rough};
+      finish_bwd_point<DIFF, SPEC>(sums, g, sc, SPEC ? r.rough[pid] : 0.f, r.g_shading + 3 * pid, pid, o);
+    }
   }
 }
 
@@ -305,22 +353,44 @@ __device__ __forceinline__ void dispatch_tile(const ReqDesc& r, int tile, const 
   }
 }
 
+// reqs: the slots' descriptors in mapped pinned host memory, written by the scheduler before the
+// first tick that names the slot; a CTA copies the descriptor of the request it works on into
+// shared memory (one read over the host link per change of request).  slot_tiles: per slot, the
+// adjoint tiles finished so far over all of the slot's requests (never reset).
+// 16-byte asynchronous copy global -> shared (cp.async, bypassing L1), and the wait for all of the
+// thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(__cvta_generic_to_global(gmem))
+               : "memory");
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __restrict__ reqs,
-                                                            const WorkList* __restrict__ wl, TickCtl* ctl) {
+                                                            const WorkList* __restrict__ wl, TickCtl* ctl,
+                                                            unsigned* __restrict__ slot_tiles,
+                                                            unsigned* __restrict__ ctrl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* s_tab = reinterpret_cast<float4*>(smem_raw);
   float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)kMaxHWpad * 32);
+  __shared__ __align__(16) ReqDesc s_desc;
   __shared__ int s_idx[2];
-  __shared__ WorkItem s_item[2];
+  __shared__ __align__(16) WorkItem s_item[2];
   __shared__ int s_last;
   const unsigned n = wl->n;
   int staged_req = -1;
   const float4* staged_table = nullptr;
-  // thread 0 fetches the index and the content of the next item one iteration ahead
+  // Thread 0 claims item indices one iteration ahead and copies the next item into shared memory
+  // with cp.async while the CTA works on the current one, so the read over the host link (the
+  // work list is mapped host memory) is off the tile's path; it waits for the copy just before
+  // the barrier that ends the iteration.
+  int claimed = 0;
   if (threadIdx.x == 0) {
     const int i0 = (int)atomicAdd(&ctl->next, 1u);
     s_idx[0] = i0;
     if (i0 < (int)n) s_item[0] = wl->items[i0];
+    claimed = (int)atomicAdd(&ctl->next, 1u);
   }
   __syncthreads();
   for (int it = 0;; ++it) {
@@ -328,46 +398,70 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
     if (idx >= (int)n) break;
     const WorkItem item = s_item[it & 1];
     if (threadIdx.x == 0) {
-      const int i1 = (int)atomicAdd(&ctl->next, 1u);
-      s_idx[(it + 1) & 1] = i1;
-      if (i1 < (int)n) s_item[(it + 1) & 1] = wl->items[i1];
+      s_idx[(it + 1) & 1] = claimed;
+      if (claimed < (int)n) cp_async16(&s_item[(it + 1) & 1], &wl->items[claimed]);
+      claimed = (int)atomicAdd(&ctl->next, 1u);
     }
     // a malformed work item is reported and skipped, never dereferenced
-    if (item.req < 0 || item.req >= kMaxSlots || (item.kind != 0 && item.kind != 1) || item.tile < 0 ||
-        (int64_t)item.tile * 32 >= reqs[item.req < 0 || item.req >= kMaxSlots ? 0 : item.req].P) {
-      if (threadIdx.x == 0) atomicOr(&reqs[0].ctrl[kCtrlError], 4u);
+    if (item.req < 0 || item.req >= kMaxSlots || (item.kind != 0 && item.kind != 1) || item.tile < 0) {
+      if (threadIdx.x == 0) {
+        atomicOr(&ctrl[kCtrlError], 4u);
+        cp_async_wait_all();
+      }
       __syncthreads();
       continue;
     }
-    const ReqDesc& r = reqs[item.req];
-    if (item.req != staged_req || r.table != staged_table) {
-      stage_table(s_tab, r.table, 0, r.HWpad);
-      staged_req = item.req;
-      staged_table = r.table;
+    if (item.req != staged_req) {
+      // plain loads, as for the work list: the host writes a slot's descriptor before it launches
+      // the first tick that names the slot.  (Loads with the .cv qualifier, which refetch system
+      // memory lines, slowed the whole kernel down several times.)
+      constexpr int kWords = (int)(sizeof(ReqDesc) / 16);
+      const uint4* src = reinterpret_cast<const uint4*>(reqs + item.req);
+      uint4* dst = reinterpret_cast<uint4*>(&s_desc);
+      if (threadIdx.x < kWords) dst[threadIdx.x] = src[threadIdx.x];
       __syncthreads();
+      staged_req = item.req;
+      if (s_desc.table != staged_table) {
+        stage_table(s_tab, s_desc.table, 0, s_desc.HWpad);
+        staged_table = s_desc.table;
+      }
+      __syncthreads();
+    }
+    const ReqDesc& r = s_desc;
+    if ((int64_t)item.tile * 32 >= r.P) {
+      if (threadIdx.x == 0) {
+        atomicOr(&ctrl[kCtrlError], 4u);
+        cp_async_wait_all();
+      }
+      __syncthreads();
+      continue;
     }
     if (item.kind == 0) {
       dispatch_tile<true>(r, item.tile, s_tab, s_red);
     } else {
       dispatch_tile<false>(r, item.tile, s_tab, s_red);
-      // the CTA that finishes a request's last adjoint tile converts its FP64 env gradient
+      // the CTA that finishes a request's last adjoint tile converts its FP64 env gradient and
+      // leaves the accumulator zeroed for its next user
       __syncthreads();
       if (threadIdx.x == 0) {
         __threadfence();
-        s_last = (atomicSub(r.bwd_tiles_left, 1u) == 1u) ? 1 : 0;
+        s_last = (atomicAdd(slot_tiles + item.req, 1u) + 1u == r.bwd_target) ? 1 : 0;
       }
       __syncthreads();
       if (s_last) {
         __threadfence();
-        for (int i = threadIdx.x; i < 3 * r.HW; i += blockDim.x) {
-          const int c = i / r.HW, t = i - c * r.HW;
-          r.g_env[i] = (float)r.env_acc[c * r.HWpad + t];
+        for (int i = threadIdx.x; i < 3 * r.HWpad; i += blockDim.x) {
+          const int c = i / r.HWpad, t = i - c * r.HWpad;
+          if (t < r.HW) r.g_env[c * r.HW + t] = (float)__ldcg(r.env_acc + i);
+          r.env_acc[i] = 0.0;
         }
       }
     }
+    if (threadIdx.x == 0) cp_async_wait_all();
     __syncthreads();
   }
-  // every CTA has made its last fetch before it counts itself out; the last one resets the tick
+  // every CTA has made its last claim before it counts itself out; the last one resets the tick
+  if (threadIdx.x == 0) __threadfence();
   if (threadIdx.x == 0 && atomicAdd(&ctl->exited, 1u) == gridDim.x - 1) {
     ctl->next = 0u;
     ctl->exited = 0u;
@@ -444,13 +538,33 @@ struct Req {
   int fwd_issued = 0, bwd_issued = 0, fwd_done = 0, bwd_done = 0;
   double cost_fwd_tile = 0, cost_bwd_tile = 0;
   ReqDesc desc{};
-  int32_t* d_perm = nullptr;         // normal-direction order (P >= kSortMinP), else null
+  int32_t* d_perm = nullptr;         // normal-direction order (see orders()), else null
+  int64_t order_min_p = 0;           // the server's ordering threshold when the request was admitted
+  double* env_acc = nullptr;         // FP64 env-gradient accumulator from the server's pool (backward)
   void* d_order_scratch = nullptr;
   // device pointers of outputs (for the download)
   float *d_shading = nullptr, *d_white = nullptr, *d_gn = nullptr, *d_gv = nullptr, *d_ga = nullptr,
         *d_gs = nullptr, *d_gr = nullptr, *d_genv = nullptr;
+  // Outputs written in place: every output the caller gave is device memory of the server's
+  // device or pinned host memory, and the batch kernel stores into those addresses (as seen from
+  // the device) instead of into the arena, so the request needs no download.
+  bool direct = false;
+  float *o_shading = nullptr, *o_white = nullptr, *o_gn = nullptr, *o_gv = nullptr, *o_ga = nullptr,
+        *o_gs = nullptr, *o_gr = nullptr, *o_genv = nullptr;
+  // Inputs read in place (device addresses of normal, view, albedo, specular, roughness, triangle
+  // ids, barycentrics, shading gradient, diffuse gradient), when inplace_in.
+  bool inplace_in = false;
+  const void* i[9] = {};
   double remaining() const {
     return (n_tiles - fwd_issued) * cost_fwd_tile + (in.backward ? (n_tiles - bwd_issued) * cost_bwd_tile : 0.0);
+  }
+  // Scheduling key (lower goes first): the remaining work, or with rank_by_size the remaining
+  // points x texels, which ranks a request asking for gradients like the same request without.
+  bool rank_by_size = false;
+  double rank() const {
+    if (!rank_by_size) return remaining();
+    const int left = in.backward ? n_tiles - std::min(fwd_issued, bwd_issued) : n_tiles - fwd_issued;
+    return left * cost_fwd_tile;
   }
 };
 
@@ -577,7 +691,7 @@ struct Mesh {
 };
 
 struct Tick {
-  double units = 0;       // work packed into the tick (pair units), for the throughput estimate
+  double units = 0;       // work packed into the tick (pair units)
   WorkList* h = nullptr;  // pinned, mapped
   WorkList* d = nullptr;  // the device's address of h
   TickCtl* ctl = nullptr;
@@ -594,20 +708,26 @@ struct Tick {
 struct des_server {
   int device = 0;
   int tick_us = 150;
-  double pairs_per_us = 0;   // throughput estimate used to size ticks (adapted to measured ticks)
-  double pairs_per_us0 = 0;  // starting estimate; the adapted value stays within 1/4x .. 4x of it
+  double pairs_per_us = 0;  // the batch kernel's throughput, which sizes the ticks
   std::atomic<int> ticks_in_flight{3};  // tick buffers in use at once (<= kNTicks)
+  std::atomic<int64_t> order_min_p{des::serve::kServeOrderMinP};  // requests with fewer points are shaded in input order
   des::serve::CopyLane up, down;
   des::serve::OrderLane order;
   unsigned char* arena_base = nullptr;
   des::serve::Arena arena;
   unsigned* d_ctrl = nullptr;
-  des::serve::ReqDesc* d_reqs = nullptr;
-  des::serve::SlotStage* h_stage = nullptr;  // pinned staging for descriptor uploads (one per slot)
+  des::serve::ReqDesc* h_desc = nullptr;  // per slot, mapped pinned host memory
+  des::serve::ReqDesc* d_desc = nullptr;  // the device's address of h_desc
+  unsigned* d_slot_tiles = nullptr;       // per slot, adjoint tiles finished (device, never reset)
+  std::vector<unsigned> slot_tiles_base;  // per slot, the counter's value once its requests are done
+  std::vector<double*> acc_pool;          // zeroed FP64 env-gradient accumulators, 3 x kMaxHWpad each
+  std::vector<void*> acc_chunks;
   std::vector<int> free_slots;
   std::vector<des::serve::Env> envs;
   std::vector<des::serve::Mesh> meshes;
-  des::serve::Tick ticks[des::serve::kNTicks];
+  des::serve::Tick ticks[des::serve::kNTicks + des::serve::kNExpress];  // normal ticks, then express ones
+  std::atomic<bool> express{false};
+  std::atomic<bool> rank_by_size{true};
   int sms = 0, grid = 0;
   size_t smem = 0;
 
@@ -616,9 +736,8 @@ struct des_server {
   std::deque<des::serve::Req*> incoming;
   std::deque<des::serve::Req*> pending;
   std::unordered_set<des::serve::Req*> active;  // admitted, not yet reported done
-  // Ready requests with tiles left to issue, by (remaining work, ticket): the scheduling order
+  // Ready requests with tiles left to issue, by (rank, ticket): the scheduling order
   std::set<std::tuple<double, int64_t, des::serve::Req*>> ready;
-  int64_t last_tick_done_ns = 0;  // completion time of the previous tick (adaptive tick sizing)
   std::vector<des_serve_done> completed;
   int64_t next_ticket = 1;
   int64_t n_submitted = 0, n_done = 0;
@@ -669,12 +788,17 @@ struct ReqLayout {
   int64_t* tri;
   int32_t* perm;
   void* order_scratch;
-  double* env_acc;
-  unsigned* tiles_left;
   size_t bytes;
 };
 
-ReqLayout request_layout(const des_serve_request& q, const Env& E, unsigned char* base) {
+// Whether the server orders a request's points by normal direction before shading it.
+inline bool orders(const des_serve_request& q, int64_t order_min_p) {
+  return q.P >= std::max(order_min_p, kSortMinP) && q.P <= kSortMaxP;
+}
+
+// inplace_in: the inputs are read where the caller keeps them (no arena copies).
+ReqLayout request_layout(const des_serve_request& q, const Env& E, int64_t order_min_p, bool inplace_in,
+                         unsigned char* base) {
   ReqLayout L{};
   size_t off = 0;
   auto take = [&](size_t n) -> unsigned char* {
@@ -683,40 +807,105 @@ ReqLayout request_layout(const des_serve_request& q, const Env& E, unsigned char
     return p;
   };
   const size_t P = (size_t)q.P;
-  L.normal = (float*)take(P * 12);
-  L.view = (float*)take(P * 12);
-  L.albedo = (float*)take(P * 12);
-  L.spec = (float*)take(P * 12);
-  L.rough = (float*)take(P * 4);
-  if (q.mesh_id >= 0) {
-    L.tri = (int64_t*)take(P * 8);
-    L.bary = (float*)take(P * 12);
+  if (!inplace_in) {
+    L.normal = (float*)take(P * 12);
+    L.view = (float*)take(P * 12);
+    L.albedo = (float*)take(P * 12);
+    L.spec = (float*)take(P * 12);
+    L.rough = (float*)take(P * 4);
+    if (q.mesh_id >= 0) {
+      L.tri = (int64_t*)take(P * 8);
+      L.bary = (float*)take(P * 12);
+    }
   }
   L.shading = (float*)take(P * 12);
   L.white = (float*)take(P * 12);
-  if (q.P >= kSortMinP && q.P <= kSortMaxP) {
+  if (orders(q, order_min_p)) {
     L.perm = (int32_t*)take(P * 4);
     L.order_scratch = take(point_order_scratch_bytes(q.P));
   }
   if (q.backward) {
-    L.gsh = (float*)take(P * 12);
-    L.gwh = (float*)take(P * 12);
+    if (!inplace_in) {
+      L.gsh = (float*)take(P * 12);
+      L.gwh = (float*)take(P * 12);
+    }
     L.grads = (float*)take(P * 12 * 4 + P * 4);
-    L.env_acc = (double*)take((size_t)3 * E.HWpad * 8);
     L.genv = (float*)take((size_t)3 * E.H * E.W * 4);
-    L.tiles_left = (unsigned*)take(256);
   }
   L.bytes = off;
   return L;
 }
 
-// Lays out the request's buffers in its arena range, fills its device descriptor and queues its
-// uploads on the upload lane (descriptor, counters and the env-gradient accumulator are set up
-// right away; the point data goes in prioritised slices).
-void upload(des_server* s, Req* r) {
+// The address under which the server's device reaches p: p for memory of that device, the
+// mapped alias for pinned host memory (*host set); null where the device cannot reach it.
+float* device_alias(const void* p, int device, bool* host) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (a.type == cudaMemoryTypeDevice && a.device == device) return static_cast<float*>(a.devicePointer);
+  if (a.type == cudaMemoryTypeHost && a.devicePointer != nullptr) {
+    *host = true;
+    return static_cast<float*>(a.devicePointer);
+  }
+  return nullptr;
+}
+
+// Resolves where the batch kernel reads and writes the request's data.  Outputs are stored in place
+// when every output it names is reachable from the device (pinned host memory only for requests
+// shaded in input order, whose tiles store whole rows).  Inputs are read in place when the request
+// is shaded in input order and every input is reachable: its tiles then fetch their points over
+// the host link themselves, and the request needs no upload.
+void resolve_request(des_server* s, Req* r) {
+  const des_serve_request& q = r->in;
+  const bool in_order = !orders(q, r->order_min_p);
+  bool host = false, ok = true;
+  auto take = [&](float* p, float** o) {
+    if (p == nullptr) return;
+    *o = device_alias(p, s->device, &host);
+    ok = ok && *o != nullptr;
+  };
+  take(q.shading, &r->o_shading);
+  take(q.diffuse_shading, &r->o_white);
+  if (q.backward) {
+    take(q.g_normal, &r->o_gn);
+    take(q.g_view_dir, &r->o_gv);
+    take(q.g_albedo, &r->o_ga);
+    take(q.g_specular_albedo, &r->o_gs);
+    take(q.g_roughness, &r->o_gr);
+    take(q.g_envmap, &r->o_genv);
+  }
+  r->direct = ok && (in_order || !host);
+  bool in_ok = in_order, in_host = false;
+  auto in = [&](const void* p, const void** o) {
+    if (p == nullptr || !in_ok) return;
+    *o = device_alias(p, s->device, &in_host);
+    in_ok = *o != nullptr;
+  };
+  in(q.normal, &r->i[0]);
+  in(q.view_dir, &r->i[1]);
+  in(q.albedo, &r->i[2]);
+  in(q.specular_albedo, &r->i[3]);
+  in(q.roughness, &r->i[4]);
+  if (q.mesh_id >= 0) {
+    in(q.nearest_triangle_id, &r->i[5]);
+    in(q.barycentric_coord, &r->i[6]);
+  }
+  if (q.backward) {
+    in(q.grad_shading, &r->i[7]);
+    in(q.grad_diffuse_shading, &r->i[8]);
+  }
+  r->inplace_in = in_ok;
+}
+
+// Lays out the request's buffers in its arena range, writes its descriptor (mapped host memory)
+// and queues its point data on the upload lane in prioritised slices.
+// Returns false when the request has nothing to upload (it is ready right away).
+bool upload(des_server* s, Req* r) {
   const des_serve_request& q = r->in;
   const Env& E = s->envs[q.env_id];
-  const ReqLayout L = request_layout(q, E, s->arena_base + r->off);
+  const ReqLayout L = request_layout(q, E, r->order_min_p, r->inplace_in, s->arena_base + r->off);
   CopyLane& lane = s->up;
   auto* job = new CopyJob();
   job->r = r;
@@ -731,42 +920,64 @@ void upload(des_server* s, Req* r) {
   d.clamp = (q.flags & DES_CLAMP) != 0;
   d.table = E.table;
   d.ctrl = s->d_ctrl;
-  job->add(L.normal, q.normal, P * 12);
-  job->add(L.view, q.view_dir, P * 12);
-  job->add(L.albedo, q.albedo, P * 12);
-  job->add(L.spec, q.specular_albedo, P * 12);
-  job->add(L.rough, q.roughness, P * 4);
-  d.normal = L.normal;
-  d.view = L.view;
-  d.albedo = L.albedo;
-  d.spec_alb = L.spec;
-  d.rough = L.rough;
+  if (r->inplace_in) {
+    d.normal = static_cast<const float*>(r->i[0]);
+    d.view = static_cast<const float*>(r->i[1]);
+    d.albedo = static_cast<const float*>(r->i[2]);
+    d.spec_alb = static_cast<const float*>(r->i[3]);
+    d.rough = static_cast<const float*>(r->i[4]);
+  } else {
+    job->add(L.normal, q.normal, P * 12);
+    job->add(L.view, q.view_dir, P * 12);
+    job->add(L.albedo, q.albedo, P * 12);
+    job->add(L.spec, q.specular_albedo, P * 12);
+    job->add(L.rough, q.roughness, P * 4);
+    d.normal = L.normal;
+    d.view = L.view;
+    d.albedo = L.albedo;
+    d.spec_alb = L.spec;
+    d.rough = L.rough;
+  }
   if (q.mesh_id >= 0) {
     const Mesh& M = s->meshes[q.mesh_id];
-    job->add(L.tri, q.nearest_triangle_id, P * 8);
-    job->add(L.bary, q.barycentric_coord, P * 12);
     d.has_vis = 1;
     d.N_face = M.N_face;
     d.N_vertex = M.N_vertex;
     d.faces = M.faces;
     d.vis = M.vis;
-    d.tri = L.tri;
-    d.bary = L.bary;
+    if (r->inplace_in) {
+      d.tri = static_cast<const int64_t*>(r->i[5]);
+      d.bary = static_cast<const float*>(r->i[6]);
+    } else {
+      job->add(L.tri, q.nearest_triangle_id, P * 8);
+      job->add(L.bary, q.barycentric_coord, P * 12);
+      d.tri = L.tri;
+      d.bary = L.bary;
+    }
   }
   r->d_shading = L.shading;
   r->d_white = L.white;
   d.shading = L.shading;
   d.white = L.white;
+  if (r->direct) {
+    d.shading = r->o_shading;
+    d.white = r->o_white;  // may be null: the kernel skips it
+  }
   if (L.perm != nullptr) {
     r->d_perm = L.perm;
     r->d_order_scratch = L.order_scratch;
     d.perm = L.perm;  // read only once the request is Ready, i.e. after its ordering
   }
   if (q.backward) {
-    job->add(L.gsh, q.grad_shading, P * 12);
-    if (q.grad_diffuse_shading) job->add(L.gwh, q.grad_diffuse_shading, P * 12);
-    d.g_shading = L.gsh;
-    d.g_white = q.grad_diffuse_shading ? L.gwh : nullptr;
+    if (r->inplace_in) {
+      d.g_shading = static_cast<const float*>(r->i[7]);
+      d.g_white = static_cast<const float*>(r->i[8]);
+    } else {
+      job->add(L.gsh, q.grad_shading, P * 12);
+      if (q.grad_diffuse_shading) job->add(L.gwh, q.grad_diffuse_shading, P * 12);
+      d.g_shading = L.gsh;
+      d.g_white = q.grad_diffuse_shading ? L.gwh : nullptr;
+    }
     r->d_gn = L.grads;
     r->d_gv = r->d_gn + 3 * P;
     r->d_ga = r->d_gv + 3 * P;
@@ -777,20 +988,29 @@ void upload(des_server* s, Req* r) {
     d.g_albedo = r->d_ga;
     d.g_spec = r->d_gs;
     d.g_rough = r->d_gr;
-    d.env_acc = L.env_acc;
+    d.env_acc = r->env_acc;
     r->d_genv = L.genv;
     d.g_env = L.genv;
-    d.bwd_tiles_left = L.tiles_left;
-    cudaMemsetAsync(d.env_acc, 0, (size_t)3 * E.HWpad * 8, lane.stream);
-    s->h_stage[r->slot].tiles_left = (unsigned)r->n_tiles;
-    cudaMemcpyAsync(d.bwd_tiles_left, &s->h_stage[r->slot].tiles_left, sizeof(unsigned), cudaMemcpyHostToDevice,
-                    lane.stream);
+    if (r->direct) {  // a null output is not written (g_normal and g_env fall back to the arena)
+      if (r->o_gn) d.g_normal = r->o_gn;
+      d.g_view = r->o_gv;
+      d.g_albedo = r->o_ga;
+      d.g_spec = r->o_gs;
+      d.g_rough = r->o_gr;
+      if (r->o_genv) d.g_env = r->o_genv;
+    }
+    s->slot_tiles_base[r->slot] += (unsigned)r->n_tiles;  // wraps like the device counter
+    d.bwd_target = s->slot_tiles_base[r->slot];
   }
-  s->h_stage[r->slot].desc = d;
-  cudaMemcpyAsync(&s->d_reqs[r->slot], &s->h_stage[r->slot].desc, sizeof(ReqDesc), cudaMemcpyHostToDevice,
-                  lane.stream);
-  job->prio = r->remaining();
+  // the descriptor goes to mapped host memory; the batch kernel reads it from there
+  s->h_desc[r->slot] = d;
+  if (job->segs.empty()) {  // inputs read in place: nothing to copy
+    delete job;
+    return false;
+  }
+  job->prio = r->rank();
   lane.queue.push_back(job);
+  return true;
 }
 
 // Queues the request's outputs on the download lane.
@@ -814,29 +1034,90 @@ void download(des_server* s, Req* r) {
   s->down.queue.push_back(job);
 }
 
+// Adds a chunk of zeroed env-gradient accumulators to the pool (at creation, then whenever more
+// backward requests are admitted at once than the pool holds).
+bool grow_acc_pool(des_server* s) {
+  constexpr int kPerChunk = 1024;
+  constexpr size_t kAcc = (size_t)3 * kMaxHWpad;  // doubles per accumulator
+  void* chunk = nullptr;
+  if (cudaMalloc(&chunk, kPerChunk * kAcc * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  // zeroed (and finished) before any request can use it
+  if (cudaMemsetAsync(chunk, 0, kPerChunk * kAcc * sizeof(double), s->order.stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->order.stream) != cudaSuccess) {
+    cudaFree(chunk);
+    return false;
+  }
+  s->acc_chunks.push_back(chunk);
+  for (int i = kPerChunk - 1; i >= 0; --i) s->acc_pool.push_back(static_cast<double*>(chunk) + i * kAcc);
+  return true;
+}
+
+// Reports a request whose outputs are in the caller's memory and frees its arena range and slot.
+void finish_request(des_server* s, Req* r, int64_t t_done) {
+  des_serve_done d{};
+  d.ticket = r->ticket;
+  d.t_submit_ns = r->t_submit - s->t0;
+  d.t_admit_ns = r->t_admit - s->t0;
+  d.t_uploaded_ns = r->t_uploaded - s->t0;
+  d.t_ready_ns = r->t_ready - s->t0;
+  d.t_computed_ns = r->t_computed - s->t0;
+  d.t_done_ns = t_done - s->t0;
+  d.status = DES_OK;
+  s->arena.release(r->off, r->bytes);
+  s->free_slots.push_back(r->slot);
+  if (r->env_acc != nullptr) s->acc_pool.push_back(r->env_acc);  // zeroed again by the last tile
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->completed.push_back(d);
+    s->n_done += 1;
+  }
+  s->cv.notify_all();
+  s->active.erase(r);
+  delete r;
+}
+
 // Builds and launches one tick if a tick buffer is free.  Returns true when work was launched.
+// When every normal tick buffer is queued on the GPU, an express buffer (a stream of the highest
+// priority, whose CTAs take the SMs before those of the queued normal ticks) takes whole requests
+// from the head of the ready set while their remaining work is at most kExpressTicks ticks, so that
+// a short request that has just become ready waits for the running tick only, not for the queued
+// ones too, and finishes within one launch.
 bool launch_tick(des_server* s) {
+  if (s->ready.empty()) return false;
   Tick* t = nullptr;
   int busy = 0;
-  for (auto& k : s->ticks) {
+  for (int i = 0; i < kNTicks; ++i) {
+    Tick& k = s->ticks[i];
     if (k.busy)
       ++busy;
     else if (t == nullptr)
       t = &k;
   }
-  if (t == nullptr || busy >= s->ticks_in_flight) return false;
-  if (s->ready.empty()) return false;
-  // shortest remaining work first, ties by arrival (the set's order)
-  const double budget = s->pairs_per_us * s->tick_us;
+  double budget = s->pairs_per_us * s->tick_us;
+  double limit = 1e300;  // remaining work of the requests this tick may take
+  if (t == nullptr || busy >= s->ticks_in_flight) {
+    t = nullptr;
+    for (int i = kNTicks; i < kNTicks + kNExpress && t == nullptr; ++i)
+      if (!s->ticks[i].busy) t = &s->ticks[i];
+    limit = kExpressTicks * budget;
+    if (!s->express || t == nullptr || std::get<0>(*s->ready.begin()) > limit) return false;
+    budget = limit;
+  }
+  // shortest remaining work first, ties by arrival (the set's order); at least one item per
+  // resident CTA while there is work, so that no SM idles for want of items
   double used = 0;
   unsigned n = 0;
+  const unsigned min_items = std::min<unsigned>((unsigned)s->grid, (unsigned)kTickItems);
+  auto room = [&] { return (used < budget || n < min_items) && n < (unsigned)kTickItems; };
   t->counts.clear();
-  while (!s->ready.empty() && used < budget && n < (unsigned)kTickItems) {
+  while (!s->ready.empty() && room() && std::get<0>(*s->ready.begin()) <= limit) {
     Req* r = std::get<2>(*s->ready.begin());
     s->ready.erase(s->ready.begin());
     int nf = 0, nb = 0;
-    while (used < budget && n < (unsigned)kTickItems && (r->fwd_issued < r->n_tiles ||
-                                                          (r->in.backward && r->bwd_issued < r->n_tiles))) {
+    while (room() && (r->fwd_issued < r->n_tiles || (r->in.backward && r->bwd_issued < r->n_tiles))) {
       // interleave forward and adjoint tiles of the same request
       if (r->fwd_issued < r->n_tiles && (!r->in.backward || r->fwd_issued <= r->bwd_issued || r->bwd_issued >= r->n_tiles)) {
         t->h->items[n++] = WorkItem{r->slot, r->fwd_issued++, 0, 0};
@@ -849,7 +1130,7 @@ bool launch_tick(des_server* s) {
       }
     }
     t->counts.push_back({r, {nf, nb}});
-    if (r->remaining() > 0) s->ready.insert({r->remaining(), r->ticket, r});  // budget is used up
+    if (r->remaining() > 0) s->ready.insert({r->rank(), r->ticket, r});  // budget is used up
   }
   t->units = used;
   t->h->n = n;
@@ -857,7 +1138,7 @@ bool launch_tick(des_server* s) {
   if (cudaGraphLaunch(t->exec, t->stream) != cudaSuccess) {
     // launch the same work without the graph
     cudaGetLastError();
-    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_reqs, t->d, t->ctl);
+    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_desc, t->d, t->ctl, s->d_slot_tiles, s->d_ctrl);
     s->stats.device_error |= 16;
   }
   count_launches(1);
@@ -910,8 +1191,15 @@ void worker_loop(des_server* s) {
     for (auto it = s->pending.begin(); it != s->pending.end();) {
       Req* r = *it;
       const Env& E = s->envs[r->in.env_id];
-      r->bytes = request_layout(r->in, E, nullptr).bytes;
+      r->order_min_p = s->order_min_p.load();
+      r->rank_by_size = s->rank_by_size.load();
+      resolve_request(s, r);
+      r->bytes = request_layout(r->in, E, r->order_min_p, r->inplace_in, nullptr).bytes;
       size_t off = 0;
+      if (r->in.backward && s->acc_pool.empty() && !grow_acc_pool(s)) {
+        ++it;
+        continue;
+      }
       if (s->free_slots.empty() || !s->arena.alloc(r->bytes, &off)) {
         ++it;
         continue;
@@ -919,14 +1207,23 @@ void worker_loop(des_server* s) {
       r->off = off;
       r->slot = s->free_slots.back();
       s->free_slots.pop_back();
+      if (r->in.backward) {
+        r->env_acc = s->acc_pool.back();
+        s->acc_pool.pop_back();
+      }
       r->t_admit = now_ns();
       r->n_tiles = (int)((r->in.P + 31) / 32);
       const double pairs = 32.0 * E.HWpad;
       r->cost_fwd_tile = pairs;
       r->cost_bwd_tile = 2.0 * pairs;
-      upload(s, r);
-      r->state = State::Uploading;
       s->active.insert(r);
+      if (upload(s, r)) {
+        r->state = State::Uploading;
+      } else {
+        r->t_uploaded = r->t_ready = r->t_admit;
+        r->state = State::Ready;
+        s->ready.insert({r->rank(), r->ticket, r});
+      }
       it = s->pending.erase(it);
       progressed = true;
       s->stats.peak_arena_bytes = std::max<int64_t>(s->stats.peak_arena_bytes, (int64_t)s->arena.used());
@@ -937,27 +1234,19 @@ void worker_loop(des_server* s) {
       const cudaError_t te = cudaEventQuery(t.done);
       if (te != cudaSuccess && te != cudaErrorNotReady) s->failed = true;
       if (te == cudaSuccess) {
-        // throughput estimate: work of this tick over the time since the previous completion,
-        // taken only while the GPU had a further tick queued (no idle gap in between)
         const int64_t tnow = now_ns();
-        int others = 0;
-        for (auto& o : s->ticks) others += (o.busy && &o != &t) ? 1 : 0;
-        if (s->last_tick_done_ns > 0 && others > 0 && t.units > 0) {
-          const double us = (tnow - s->last_tick_done_ns) * 1e-3;
-          if (us > 5.0) {
-            const double rate = std::min(std::max(t.units / us, 0.25 * s->pairs_per_us0), 4.0 * s->pairs_per_us0);
-            s->pairs_per_us = 0.9 * s->pairs_per_us + 0.1 * rate;
-          }
-        }
-        s->last_tick_done_ns = tnow;
         for (auto& c : t.counts) {
           Req* r = c.first;
           r->fwd_done += c.second.first;
           r->bwd_done += c.second.second;
           if (r->state == State::Ready && r->fwd_done == r->n_tiles && (!r->in.backward || r->bwd_done == r->n_tiles)) {
             r->t_computed = tnow;
-            download(s, r);
-            r->state = State::Downloading;
+            if (r->direct) {  // outputs are already in place
+              finish_request(s, r, tnow);
+            } else {
+              download(s, r);
+              r->state = State::Downloading;
+            }
           }
         }
         t.counts.clear();
@@ -983,14 +1272,11 @@ void worker_loop(des_server* s) {
       } else {
         if (r->d_perm != nullptr) {  // no ordering after all: shade in input order
           r->desc.perm = nullptr;
-          s->h_stage[r->slot].desc.perm = nullptr;
-          cudaMemcpyAsync(&s->d_reqs[r->slot].perm, &s->h_stage[r->slot].desc.perm, sizeof(void*),
-                          cudaMemcpyHostToDevice, s->order.stream);
-          cudaStreamSynchronize(s->order.stream);
+          s->h_desc[r->slot].perm = nullptr;  // no tick has read the descriptor yet
         }
         r->state = State::Ready;
         r->t_ready = now_ns();
-        s->ready.insert({r->remaining(), r->ticket, r});
+        s->ready.insert({r->rank(), r->ticket, r});
       }
     }
     while (!s->order.flight.empty()) {
@@ -1005,7 +1291,7 @@ void worker_loop(des_server* s) {
       s->order.flight.pop_front();
       r->state = State::Ready;
       r->t_ready = now_ns();
-      s->ready.insert({r->remaining(), r->ticket, r});
+      s->ready.insert({r->rank(), r->ticket, r});
       progressed = true;
     }
     fin.clear();
@@ -1014,25 +1300,7 @@ void worker_loop(des_server* s) {
       Req* r = j->r;
       delete j;
       progressed = true;
-      des_serve_done d{};
-      d.ticket = r->ticket;
-      d.t_submit_ns = r->t_submit - s->t0;
-      d.t_admit_ns = r->t_admit - s->t0;
-      d.t_uploaded_ns = r->t_uploaded - s->t0;
-      d.t_ready_ns = r->t_ready - s->t0;
-      d.t_computed_ns = r->t_computed - s->t0;
-      d.t_done_ns = now_ns() - s->t0;
-      d.status = DES_OK;
-      s->arena.release(r->off, r->bytes);
-      s->free_slots.push_back(r->slot);
-      {
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->completed.push_back(d);
-        s->n_done += 1;
-      }
-      s->cv.notify_all();
-      s->active.erase(r);
-      delete r;
+      finish_request(s, r, now_ns());
     }
     // 4. new ticks, new copies
     while (launch_tick(s)) progressed = true;
@@ -1074,20 +1342,27 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
   }
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
   // a conservative starting throughput; it only sizes ticks
-  s->pairs_per_us = 1.5e5 * s->sms / 148.0;
-  s->pairs_per_us0 = s->pairs_per_us;
+  s->pairs_per_us = des::serve::kBatchPairsPerUs * s->sms / 148.0;
   bool ok = s->up.init(cudaMemcpyHostToDevice, size_t(1) << 20, size_t(4) << 20) &&
             s->down.init(cudaMemcpyDeviceToHost, size_t(1) << 20, size_t(4) << 20) && s->order.init() &&
             cudaMalloc(&s->arena_base, hbm_budget_bytes) == cudaSuccess &&
             cudaMalloc(&s->d_ctrl, 256) == cudaSuccess &&
-            cudaMalloc(&s->d_reqs, sizeof(des::serve::ReqDesc) * des::serve::kMaxSlots) == cudaSuccess &&
-            cudaMallocHost(&s->h_stage, sizeof(des::serve::SlotStage) * des::serve::kMaxSlots) == cudaSuccess &&
+            cudaHostAlloc(&s->h_desc, sizeof(des::serve::ReqDesc) * des::serve::kMaxSlots, cudaHostAllocMapped) ==
+                cudaSuccess &&
+            cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_desc), s->h_desc, 0) == cudaSuccess &&
+            cudaMalloc(&s->d_slot_tiles, sizeof(unsigned) * des::serve::kMaxSlots) == cudaSuccess &&
+            cudaMemset(s->d_slot_tiles, 0, sizeof(unsigned) * des::serve::kMaxSlots) == cudaSuccess &&
             cudaMemset(s->d_ctrl, 0, 256) == cudaSuccess;
   if (!ok) {
     des_server_destroy(s);
     return DES_ERR_CUDA;
   }
   s->arena.init(hbm_budget_bytes);
+  s->slot_tiles_base.assign(des::serve::kMaxSlots, 0u);
+  if (!des::serve::grow_acc_pool(s)) {
+    des_server_destroy(s);
+    return DES_ERR_CUDA;
+  }
   for (int i = des::serve::kMaxSlots - 1; i >= 0; --i) s->free_slots.push_back(i);
   s->smem = (size_t)des::serve::kMaxHWpad * 32 + (size_t)des::serve::kNW * 15 * 32 * 4;
   if (cudaFuncSetAttribute(des::serve::batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem) !=
@@ -1099,12 +1374,15 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, des::serve::batch_kernel, des::serve::kNW * 32, s->smem);
   s->grid = std::max(1, occ) * s->sms;
   // one captured graph per tick buffer: the persistent batch kernel over that buffer's work list
+  int least_prio = 0, greatest_prio = 0;
+  cudaDeviceGetStreamPriorityRange(&least_prio, &greatest_prio);
   for (auto& t : s->ticks) {
+    const int prio = (&t >= &s->ticks[des::serve::kNTicks]) ? greatest_prio : least_prio;
     ok = cudaHostAlloc(&t.h, sizeof(des::serve::WorkList), cudaHostAllocMapped) == cudaSuccess &&
          cudaHostGetDevicePointer(reinterpret_cast<void**>(&t.d), t.h, 0) == cudaSuccess &&
          cudaMalloc(&t.ctl, sizeof(des::serve::TickCtl)) == cudaSuccess &&
          cudaMemset(t.ctl, 0, sizeof(des::serve::TickCtl)) == cudaSuccess &&
-         cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaStreamCreateWithPriority(&t.stream, cudaStreamNonBlocking, prio) == cudaSuccess &&
          cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming) == cudaSuccess &&
          cudaDeviceSynchronize() == cudaSuccess;
     if (!ok) {
@@ -1114,7 +1392,8 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
     std::memset(t.h, 0, sizeof(des::serve::WorkList));
     cudaGraph_t g = nullptr;
     ok = cudaStreamBeginCapture(t.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    des::serve::batch_kernel<<<s->grid, des::serve::kNW * 32, s->smem, t.stream>>>(s->d_reqs, t.d, t.ctl);
+    des::serve::batch_kernel<<<s->grid, des::serve::kNW * 32, s->smem, t.stream>>>(s->d_desc, t.d, t.ctl,
+                                                                                   s->d_slot_tiles, s->d_ctrl);
     ok = ok && cudaStreamEndCapture(t.stream, &g) == cudaSuccess;
     ok = ok && cudaGraphInstantiate(&t.exec, g, 0) == cudaSuccess;
     if (g) cudaGraphDestroy(g);
@@ -1229,6 +1508,24 @@ int des_server_set_ticks_in_flight(des_server* s, int n) {
   return DES_OK;
 }
 
+int des_server_set_rank_by_size(des_server* s, int enable) {
+  if (s == nullptr) return DES_ERR_INVALID_ARGUMENT;
+  s->rank_by_size = enable != 0;
+  return DES_OK;
+}
+
+int des_server_set_express(des_server* s, int enable) {
+  if (s == nullptr) return DES_ERR_INVALID_ARGUMENT;
+  s->express = enable != 0;
+  return DES_OK;
+}
+
+int des_server_set_order_min_points(des_server* s, int64_t n) {
+  if (s == nullptr || n < 0) return DES_ERR_INVALID_ARGUMENT;
+  s->order_min_p = n;
+  return DES_OK;
+}
+
 int des_server_stats(des_server* s, des_serve_stats* out) {
   if (s == nullptr || out == nullptr) return DES_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(s->mu);
@@ -1263,8 +1560,9 @@ int des_server_destroy(des_server* s) {
   }
   for (Req* r : s->pending) delete r;
   for (Req* r : s->incoming) delete r;
-  if (s->h_stage) cudaFreeHost(s->h_stage);
-  if (s->d_reqs) cudaFree(s->d_reqs);
+  if (s->h_desc) cudaFreeHost(s->h_desc);
+  if (s->d_slot_tiles) cudaFree(s->d_slot_tiles);
+  for (void* c : s->acc_chunks) cudaFree(c);
   if (s->d_ctrl) cudaFree(s->d_ctrl);
   if (s->arena_base) cudaFree(s->arena_base);
   s->up.destroy();

@@ -11,6 +11,7 @@ U[0.2,0.9] roughness, U[0,0.1] specular).  Point data comes from a few pre-gener
 
 Latency of a request = time its outputs are in host memory - its arrival time.
 """
+import gc
 import math
 import time
 
@@ -98,14 +99,19 @@ def _summarize(lat_s, sched, makespan_s):
 
 
 def run_served(pools, sched, bary, device=0, hbm_budget_bytes=40 << 30, tick_us=75, ticks_in_flight=None,
-               trace=False):
+               trace=False, order_min_points=None, express=None, rank_by_size=None):
     from .serving import Server
-    srv = Server(device=device, hbm_budget_bytes=hbm_budget_bytes, tick_us=tick_us, ticks_in_flight=ticks_in_flight)
+    srv = Server(device=device, hbm_budget_bytes=hbm_budget_bytes, tick_us=tick_us, ticks_in_flight=ticks_in_flight,
+                 order_min_points=order_min_points, express=express, rank_by_size=rank_by_size)
     try:
         env_ids = {k: [srv.add_envmap(e) for e in v] for k, v in pools.envs.items()}
         mesh_ids = [srv.add_mesh(f, b) for f, b in pools.meshes]
         torch.cuda.synchronize()
         reqs = [None] * len(sched)
+        # no collector pause inside the arrival loop (a full collection stalls submission for tens
+        # of milliseconds and turns the Poisson schedule into a burst)
+        gc.collect()
+        gc.disable()
         t0 = time.perf_counter()
         for i, r in enumerate(sched):
             while time.perf_counter() - t0 < r["t"]:
@@ -128,6 +134,7 @@ def run_served(pools, sched, bary, device=0, hbm_budget_bytes=40 << 30, tick_us=
         srv.poll(len(sched) + 16)
         stats = srv.stats()
     finally:
+        gc.enable()
         srv.close()
     bad = [q.status for q in reqs if q.status != 0]
     if bad:
@@ -166,6 +173,8 @@ def run_serial_plain(pools, sched, bary, device=0):
     meshes = [(f.to(dev), b.to(dev)) for f, b in pools.meshes]
     R = torch.eye(3, device=dev)
     lat = []
+    gc.collect()
+    gc.disable()
     t0 = time.perf_counter()
     first = None
     for i, r in enumerate(sched):
@@ -201,6 +210,7 @@ def run_serial_plain(pools, sched, bary, device=0):
                 host[k][:P].copy_(o, non_blocking=True)
         torch.cuda.synchronize(dev)
         lat.append(time.perf_counter() - t0 - r["t"])
+    gc.enable()
     makespan = time.perf_counter() - first
     return _summarize(lat, sched, makespan)
 

@@ -64,9 +64,13 @@ def _load():
         L.des_server_stats.argtypes = [_vp, ctypes.POINTER(_Stats)]
         L.des_server_destroy.argtypes = [_vp]
         L.des_server_set_ticks_in_flight.argtypes = [_vp, ctypes.c_int]
+        L.des_server_set_order_min_points.argtypes = [_vp, ctypes.c_int64]
+        L.des_server_set_express.argtypes = [_vp, ctypes.c_int]
+        L.des_server_set_rank_by_size.argtypes = [_vp, ctypes.c_int]
         for f in ("des_server_create", "des_server_add_envmap", "des_server_add_mesh", "des_server_submit",
                   "des_server_poll", "des_server_drain", "des_server_stats", "des_server_destroy",
-                  "des_server_set_ticks_in_flight"):
+                  "des_server_set_ticks_in_flight", "des_server_set_order_min_points", "des_server_set_express",
+                  "des_server_set_rank_by_size"):
             getattr(L, f).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -81,9 +85,12 @@ def _ptr(t):
     return None if t is None else _vp(t.data_ptr())
 
 
-def _host(t, dtype):
-    """Contiguous pinned host tensor of dtype (copies only when needed)."""
+def _host(t, dtype, device=None):
+    """Contiguous tensor of dtype that the server can read: a CUDA tensor on `device` stays where it
+    is, anything else becomes pinned host memory (copies only when needed)."""
     t = t.detach()
+    if device is not None and t.is_cuda and t.device.index == device:
+        return t.to(dtype).contiguous()
     if t.device.type != "cpu" or t.dtype != dtype or not t.is_contiguous() or not t.is_pinned():
         t = t.to("cpu", dtype).contiguous().pin_memory()
     return t
@@ -103,7 +110,8 @@ class Request:
 
 
 class Server:
-    def __init__(self, device=0, hbm_budget_bytes=40 << 30, tick_us=150, ticks_in_flight=None):
+    def __init__(self, device=0, hbm_budget_bytes=40 << 30, tick_us=150, ticks_in_flight=None,
+                 order_min_points=None, express=None, rank_by_size=None):
         self._L = _load()
         h = _vp()
         _check(self._L.des_server_create(int(device), int(hbm_budget_bytes), int(tick_us), ctypes.byref(h)),
@@ -111,6 +119,14 @@ class Server:
         self._h = h
         if ticks_in_flight is not None:
             _check(self._L.des_server_set_ticks_in_flight(h, int(ticks_in_flight)), "des_server_set_ticks_in_flight")
+        if rank_by_size is not None:
+            _check(self._L.des_server_set_rank_by_size(h, int(bool(rank_by_size))), "des_server_set_rank_by_size")
+        if express is not None:
+            _check(self._L.des_server_set_express(h, int(bool(express))), "des_server_set_express")
+        if order_min_points is not None:
+            _check(self._L.des_server_set_order_min_points(h, int(order_min_points)),
+                   "des_server_set_order_min_points")
+        self._device = int(device)
         self._envs = {}
         self._requests = {}
 
@@ -134,20 +150,23 @@ class Server:
     def submit(self, normal, view_dir, albedo, specular_albedo, roughness, env_id, mesh_id=-1,
                nearest_triangle_id=None, barycentric_coord=None, backward=False, grad_shading=None,
                grad_diffuse_shading=None, enable_specular=True, outputs=None):
-        """Queues one request.  Inputs are host tensors (copied to pinned memory if they are not);
-        `outputs` optionally supplies pinned host output tensors to write into."""
+        """Queues one request.  Inputs are pinned host tensors or CUDA tensors on the server's
+        device (anything else is copied to pinned memory first); `outputs` optionally supplies output
+        tensors to write into (pinned or pageable host tensors, or CUDA tensors on the server's
+        device).  Inputs and outputs must stay untouched until the request is done."""
         P = normal.shape[0]
         H, W = self._envs[env_id]
-        ins = {k: _host(v, torch.float32) for k, v in (("normal", normal), ("view_dir", view_dir), ("albedo", albedo),
-                                                        ("specular_albedo", specular_albedo),
-                                                        ("roughness", roughness))}
+        dv = self._device
+        ins = {k: _host(v, torch.float32, dv) for k, v in (("normal", normal), ("view_dir", view_dir),
+                                                            ("albedo", albedo), ("specular_albedo", specular_albedo),
+                                                            ("roughness", roughness))}
         if mesh_id >= 0:
-            ins["nearest_triangle_id"] = _host(nearest_triangle_id, torch.int64)
-            ins["barycentric_coord"] = _host(barycentric_coord, torch.float32)
+            ins["nearest_triangle_id"] = _host(nearest_triangle_id, torch.int64, dv)
+            ins["barycentric_coord"] = _host(barycentric_coord, torch.float32, dv)
         if backward:
-            ins["grad_shading"] = _host(grad_shading, torch.float32)
+            ins["grad_shading"] = _host(grad_shading, torch.float32, dv)
             if grad_diffuse_shading is not None:
-                ins["grad_diffuse_shading"] = _host(grad_diffuse_shading, torch.float32)
+                ins["grad_diffuse_shading"] = _host(grad_diffuse_shading, torch.float32, dv)
         if outputs is None:
             pin = dict(dtype=torch.float32, pin_memory=True)
             outputs = {"shading": torch.empty(P, 3, **pin), "diffuse_shading": torch.empty(P, 3, **pin)}

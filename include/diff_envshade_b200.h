@@ -209,15 +209,35 @@ int des_server_add_envmap(des_server* s, int32_t H, int32_t W, const float* envm
 int des_server_add_mesh(des_server* s, int32_t N_face, int32_t N_vertex, int32_t N_slot,
                         const int32_t* face_vertex_list, const int32_t* visibility, int32_t* mesh_id);
 /* Queues a request; returns immediately with its ticket.  After a CUDA error the server fails every
- * outstanding request (status DES_ERR_CUDA in des_serve_done) and refuses new ones. */
+ * outstanding request (status DES_ERR_CUDA in des_serve_done) and refuses new ones.  When every
+ * output the request names is device memory of the server's device, or pinned host memory and the
+ * request is shaded in input order, the batch kernel stores the results there directly; otherwise
+ * they are staged in the arena and copied back.  Either way they are in place when the request is
+ * reported done.  A request shaded in input order whose inputs are all device memory of the
+ * server's device or pinned host memory is read in place (no upload); other requests' inputs are
+ * copied into the arena.  The caller keeps every buffer valid and unchanged until the request is
+ * reported done. */
 int des_server_submit(des_server* s, const des_serve_request* req, int64_t* ticket);
-/* Moves up to max_items finished requests (outputs already in host memory) into out[]. */
+/* Moves up to max_items finished requests (outputs already in the caller's memory) into out[]. */
 int des_server_poll(des_server* s, des_serve_done* out, int max_items, int* count);
 /* Waits until every submitted request has finished (DES_ERR_TIMEOUT after timeout_ms). */
 int des_server_drain(des_server* s, int timeout_ms);
 /* How many ticks may be queued on the GPU at once (1..4, default 3): more overlaps consecutive
  * ticks better, fewer lets a newly arrived request start sooner. */
 int des_server_set_ticks_in_flight(des_server* s, int n);
+/* Requests of at least n points (and at least 16384) are ordered by normal direction before they
+ * are shaded; smaller ones are shaded in input order (by default no request is ordered).  Applies
+ * to requests admitted after the call. */
+int des_server_set_order_min_points(des_server* s, int64_t n);
+/* Scheduling order of the ready requests (and of their uploads): least remaining points x texels
+ * first (enable = 1, the default), which ranks a request that asks for gradients like the same
+ * request without them, or least remaining work first (enable = 0).  Applies to requests admitted
+ * after the call. */
+int des_server_set_rank_by_size(des_server* s, int enable);
+/* Express ticks on or off (default off): while every normal tick is queued on the GPU, requests
+ * with at most six ticks of work left go whole into an extra tick (two at most at a time) on a
+ * stream of the highest priority, which starts as soon as the running tick's CTAs finish. */
+int des_server_set_express(des_server* s, int enable);
 int des_server_stats(des_server* s, des_serve_stats* out);
 /* Finishes queued work and frees the server. */
 int des_server_destroy(des_server* s);

@@ -150,3 +150,49 @@ def test_admission_respects_hbm_budget():
     assert 0 < st["peak_arena_bytes"] <= budget
     # admission had to wait for memory: some request was admitted well after it was submitted
     assert max(r.done[1] - r.done[0] for r in reqs) > 0
+
+
+def _outputs(P, H, W, where):
+    kw = {"pinned": dict(pin_memory=True), "pageable": {}, "device": dict(device="cuda")}[where]
+    o = {k: torch.empty(P, 3, **kw) for k in ("shading", "diffuse_shading", "g_normal", "g_view_dir", "g_albedo",
+                                               "g_specular_albedo")}
+    o["g_roughness"] = torch.empty(P, 1, **kw)
+    o["g_envmap"] = torch.empty(3, H, W, **kw)
+    return o
+
+
+def test_outputs_in_place_and_staged_agree():
+    """Outputs given as device memory or pinned host memory are stored in place by the batch
+    kernel; pageable host outputs (and pinned ones of an ordered request) are staged in the arena
+    and copied back.  Inputs of a request in input order are read in place (pinned host or device
+    memory); an ordered request's inputs are uploaded.  Every placement, ordered or not, gives the
+    same per-point results."""
+    from diff_envshade_b200.serving import Server
+    g = torch.Generator().manual_seed(21)
+    faces, vis_bits = _mesh(12)
+    env = torch.exp(torch.randn(3, 16, 32, generator=g))
+    inp, tri, bary = _points(40000, seed=40, N_face=faces.shape[1])
+    results = {}
+    for order_min in (1 << 30, 16384):  # input order, then normal-direction order
+        with Server(device=0, hbm_budget_bytes=1 << 30, tick_us=100, order_min_points=order_min) as srv:
+            env_id = srv.add_envmap(env)
+            mesh_id = srv.add_mesh(faces, vis_bits)
+            for src, where in (("host", "pinned"), ("host", "pageable"), ("host", "device"), ("device", "pinned"),
+                               ("device", "device")):
+                d = inp.to("cuda") if src == "device" else inp
+                t, b = (tri.cuda(), bary.cuda()) if src == "device" else (tri, bary)
+                outs = _outputs(inp.P, 16, 32, where)
+                req = srv.submit(d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness,
+                                 env_id=env_id, mesh_id=mesh_id, nearest_triangle_id=t, barycentric_coord=b,
+                                 backward=True, grad_shading=d.grad_shading,
+                                 grad_diffuse_shading=d.grad_diffuse_shading, outputs=outs)
+                srv.drain(60)
+                srv.poll()
+                assert req.status == 0
+                torch.cuda.synchronize()
+                results[(order_min, src, where)] = {k: v.cpu() for k, v in outs.items()}
+            assert srv.stats()["device_error"] == 0
+    ref = results[(1 << 30, "host", "pageable")]
+    for key, got in results.items():
+        _compare(got, ref, f"{key}", exact=True)
+        assert_close_grad(got["g_envmap"], ref["g_envmap"], f"{key}:g_envmap")
