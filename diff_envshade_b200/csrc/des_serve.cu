@@ -13,8 +13,7 @@
 //   * every tick packs 32-point tiles of the admitted requests into a work list, smallest
 //     remaining work first, up to a time budget, into a work list in mapped pinned memory and
 //     launches it as a CUDA graph (one persistent batch kernel) on its own stream, with up to
-//     ticks_in_flight ticks queued so that consecutive ticks overlap, plus an express tick on a
-//     high-priority stream for short requests that become ready while the normal ticks are queued;
+//     ticks_in_flight ticks queued so that consecutive ticks overlap;
 //   * when every tile of a request has finished, copies its outputs back and frees its memory.
 // Work of different requests therefore shares each launch and each SM; a request that arrives
 // while others run joins the next tick.
@@ -26,7 +25,10 @@
 // The batch kernel evaluates exactly the per-pair arithmetic of des_fwd_kernel / des_bwd_kernel
 // (shared helpers in des_point.cuh); per-point outputs are bit-identical to a solo call of the
 // batch path, and the env-map gradient is summed per request in FP64 (global FP64 atomics, then a
-// final FP32 conversion by whichever CTA finishes the request's last adjoint tile).
+// final FP32 conversion by whichever CTA finishes the request's last adjoint tile).  A request with
+// gradients runs adjoint tiles only: the adjoint integrates the forward weights too, and its sums
+// give the request's shading (equal to a forward tile's within rounding), a third less work than
+// running both.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -57,9 +59,7 @@ constexpr int kNW = 8;               // warps per CTA
 constexpr int kMaxHWpad = 2048;      // texel table kept in shared memory per CTA
 constexpr int kMaxSlots = 8192;      // concurrently admitted requests
 constexpr int kTickItems = 4096;     // work items per tick (upper bound; the whole list is uploaded)
-constexpr int kNTicks = 4;           // normal tick buffers (up to this many ticks in flight)
-constexpr int kNExpress = 2;         // express tick buffers (after the normal ones), highest priority
-constexpr double kExpressTicks = 6;  // express ticks take requests with at most this many ticks of work
+constexpr int kNTicks = 4;           // tick buffers (up to this many ticks in flight)
 constexpr int kCopyEvents = 64;                    // completion events per copy lane
 // Default ordering threshold of the server (requests of at least this many points are ordered by
 // normal direction): none.  An ordered request must be uploaded (the ordering kernels and the
@@ -220,6 +220,21 @@ __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
   }
 }
 
+// A point's forward outputs from the adjoint's sums: sums[0..2] = sum of wd L_c (the diffuse
+// shading), sums[3..5] = sum of ws L_c, the forward tile's accumulators integrated over the same
+// texels in the same order (the pair weights are rounded in another association, so the outputs
+// equal a forward tile's within rounding).
+template <bool DIFF, bool SPEC>
+__device__ __forceinline__ void fwd_outputs(const ReqDesc& r, int64_t pid, bool valid, const float (&sums)[15],
+                                            float (&out)[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    out[c] = 0.f;
+    if (DIFF) out[c] = (valid ? r.albedo[3 * pid + c] : 0.f) * sums[c];
+    if (SPEC) out[c] = fmaf(valid ? r.spec_alb[3 * pid + c] : 0.f, sums[3 + c], out[c]);
+  }
+}
+
 template <bool DIFF, bool SPEC, bool VIS>
 __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
   constexpr int NACC = 15;
@@ -320,12 +335,23 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
                   g2 = valid ? r.g_shading[3 * pid + 2] : 0.f;
       const BwdGrads q = bwd_point_grads<DIFF, SPEC>(sums, g, sc, rough, g0, g1, g2);
       const int64_t first = (int64_t)tile * 32;
+      float out[3];
+      fwd_outputs<DIFF, SPEC>(r, pid, valid, sums, out);
+      store_rows3(r.shading, first, r.P, out[0], out[1], out[2], lane);
+      if (r.white != nullptr) store_rows3(r.white, first, r.P, sums[0], sums[1], sums[2], lane);
       store_rows3(r.g_normal, first, r.P, q.n[0], q.n[1], q.n[2], lane);
       if (r.g_albedo != nullptr) store_rows3(r.g_albedo, first, r.P, q.a[0], q.a[1], q.a[2], lane);
       if (r.g_spec != nullptr) store_rows3(r.g_spec, first, r.P, q.s[0], q.s[1], q.s[2], lane);
       if (r.g_view != nullptr) store_rows3(r.g_view, first, r.P, q.v[0], q.v[1], q.v[2], lane);
       if (r.g_rough != nullptr && valid) r.g_rough[pid] = q.rough;
     } else if (valid) {
+      float out[3];
+      fwd_outputs<DIFF, SPEC>(r, pid, valid, sums, out);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        r.shading[3 * pid + c] = out[c];
+        if (r.white != nullptr) r.white[3 * pid + c] = sums[c];
+      }
       const BwdOutputs o{r.g_normal, r.g_view, r.g_albedo, r.g_spec, r.g_rough};
       finish_bwd_point<DIFF, SPEC>(sums, g, sc, SPEC ? r.rough[pid] : 0.f, r.g_shading + 3 * pid, pid, o);
     }
@@ -725,8 +751,7 @@ struct des_server {
   std::vector<int> free_slots;
   std::vector<des::serve::Env> envs;
   std::vector<des::serve::Mesh> meshes;
-  des::serve::Tick ticks[des::serve::kNTicks + des::serve::kNExpress];  // normal ticks, then express ones
-  std::atomic<bool> express{false};
+  des::serve::Tick ticks[des::serve::kNTicks];
   std::atomic<bool> rank_by_size{true};
   int sms = 0, grid = 0;
   size_t smem = 0;
@@ -1080,32 +1105,18 @@ void finish_request(des_server* s, Req* r, int64_t t_done) {
 }
 
 // Builds and launches one tick if a tick buffer is free.  Returns true when work was launched.
-// When every normal tick buffer is queued on the GPU, an express buffer (a stream of the highest
-// priority, whose CTAs take the SMs before those of the queued normal ticks) takes whole requests
-// from the head of the ready set while their remaining work is at most kExpressTicks ticks, so that
-// a short request that has just become ready waits for the running tick only, not for the queued
-// ones too, and finishes within one launch.
 bool launch_tick(des_server* s) {
   if (s->ready.empty()) return false;
   Tick* t = nullptr;
   int busy = 0;
-  for (int i = 0; i < kNTicks; ++i) {
-    Tick& k = s->ticks[i];
+  for (auto& k : s->ticks) {
     if (k.busy)
       ++busy;
     else if (t == nullptr)
       t = &k;
   }
-  double budget = s->pairs_per_us * s->tick_us;
-  double limit = 1e300;  // remaining work of the requests this tick may take
-  if (t == nullptr || busy >= s->ticks_in_flight) {
-    t = nullptr;
-    for (int i = kNTicks; i < kNTicks + kNExpress && t == nullptr; ++i)
-      if (!s->ticks[i].busy) t = &s->ticks[i];
-    limit = kExpressTicks * budget;
-    if (!s->express || t == nullptr || std::get<0>(*s->ready.begin()) > limit) return false;
-    budget = limit;
-  }
+  if (t == nullptr || busy >= s->ticks_in_flight) return false;
+  const double budget = s->pairs_per_us * s->tick_us;
   // shortest remaining work first, ties by arrival (the set's order); at least one item per
   // resident CTA while there is work, so that no SM idles for want of items
   double used = 0;
@@ -1113,7 +1124,7 @@ bool launch_tick(des_server* s) {
   const unsigned min_items = std::min<unsigned>((unsigned)s->grid, (unsigned)kTickItems);
   auto room = [&] { return (used < budget || n < min_items) && n < (unsigned)kTickItems; };
   t->counts.clear();
-  while (!s->ready.empty() && room() && std::get<0>(*s->ready.begin()) <= limit) {
+  while (!s->ready.empty() && room()) {
     Req* r = std::get<2>(*s->ready.begin());
     s->ready.erase(s->ready.begin());
     int nf = 0, nb = 0;
@@ -1213,6 +1224,8 @@ void worker_loop(des_server* s) {
       }
       r->t_admit = now_ns();
       r->n_tiles = (int)((r->in.P + 31) / 32);
+      // a request with gradients runs adjoint tiles only: they store its forward outputs too
+      if (r->in.backward) r->fwd_issued = r->fwd_done = r->n_tiles;
       const double pairs = 32.0 * E.HWpad;
       r->cost_fwd_tile = pairs;
       r->cost_bwd_tile = 2.0 * pairs;
@@ -1374,15 +1387,12 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, des::serve::batch_kernel, des::serve::kNW * 32, s->smem);
   s->grid = std::max(1, occ) * s->sms;
   // one captured graph per tick buffer: the persistent batch kernel over that buffer's work list
-  int least_prio = 0, greatest_prio = 0;
-  cudaDeviceGetStreamPriorityRange(&least_prio, &greatest_prio);
   for (auto& t : s->ticks) {
-    const int prio = (&t >= &s->ticks[des::serve::kNTicks]) ? greatest_prio : least_prio;
     ok = cudaHostAlloc(&t.h, sizeof(des::serve::WorkList), cudaHostAllocMapped) == cudaSuccess &&
          cudaHostGetDevicePointer(reinterpret_cast<void**>(&t.d), t.h, 0) == cudaSuccess &&
          cudaMalloc(&t.ctl, sizeof(des::serve::TickCtl)) == cudaSuccess &&
          cudaMemset(t.ctl, 0, sizeof(des::serve::TickCtl)) == cudaSuccess &&
-         cudaStreamCreateWithPriority(&t.stream, cudaStreamNonBlocking, prio) == cudaSuccess &&
+         cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking) == cudaSuccess &&
          cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming) == cudaSuccess &&
          cudaDeviceSynchronize() == cudaSuccess;
     if (!ok) {
@@ -1511,12 +1521,6 @@ int des_server_set_ticks_in_flight(des_server* s, int n) {
 int des_server_set_rank_by_size(des_server* s, int enable) {
   if (s == nullptr) return DES_ERR_INVALID_ARGUMENT;
   s->rank_by_size = enable != 0;
-  return DES_OK;
-}
-
-int des_server_set_express(des_server* s, int enable) {
-  if (s == nullptr) return DES_ERR_INVALID_ARGUMENT;
-  s->express = enable != 0;
   return DES_OK;
 }
 

@@ -99,10 +99,10 @@ def _summarize(lat_s, sched, makespan_s):
 
 
 def run_served(pools, sched, bary, device=0, hbm_budget_bytes=40 << 30, tick_us=75, ticks_in_flight=None,
-               trace=False, order_min_points=None, express=None, rank_by_size=None):
+               trace=False, order_min_points=None, rank_by_size=None):
     from .serving import Server
     srv = Server(device=device, hbm_budget_bytes=hbm_budget_bytes, tick_us=tick_us, ticks_in_flight=ticks_in_flight,
-                 order_min_points=order_min_points, express=express, rank_by_size=rank_by_size)
+                 order_min_points=order_min_points, rank_by_size=rank_by_size)
     try:
         env_ids = {k: [srv.add_envmap(e) for e in v] for k, v in pools.envs.items()}
         mesh_ids = [srv.add_mesh(f, b) for f, b in pools.meshes]

@@ -65,12 +65,10 @@ def _load():
         L.des_server_destroy.argtypes = [_vp]
         L.des_server_set_ticks_in_flight.argtypes = [_vp, ctypes.c_int]
         L.des_server_set_order_min_points.argtypes = [_vp, ctypes.c_int64]
-        L.des_server_set_express.argtypes = [_vp, ctypes.c_int]
         L.des_server_set_rank_by_size.argtypes = [_vp, ctypes.c_int]
         for f in ("des_server_create", "des_server_add_envmap", "des_server_add_mesh", "des_server_submit",
                   "des_server_poll", "des_server_drain", "des_server_stats", "des_server_destroy",
-                  "des_server_set_ticks_in_flight", "des_server_set_order_min_points", "des_server_set_express",
-                  "des_server_set_rank_by_size"):
+                  "des_server_set_ticks_in_flight", "des_server_set_order_min_points", "des_server_set_rank_by_size"):
             getattr(L, f).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -111,7 +109,7 @@ class Request:
 
 class Server:
     def __init__(self, device=0, hbm_budget_bytes=40 << 30, tick_us=150, ticks_in_flight=None,
-                 order_min_points=None, express=None, rank_by_size=None):
+                 order_min_points=None, rank_by_size=None):
         self._L = _load()
         h = _vp()
         _check(self._L.des_server_create(int(device), int(hbm_budget_bytes), int(tick_us), ctypes.byref(h)),
@@ -121,8 +119,6 @@ class Server:
             _check(self._L.des_server_set_ticks_in_flight(h, int(ticks_in_flight)), "des_server_set_ticks_in_flight")
         if rank_by_size is not None:
             _check(self._L.des_server_set_rank_by_size(h, int(bool(rank_by_size))), "des_server_set_rank_by_size")
-        if express is not None:
-            _check(self._L.des_server_set_express(h, int(bool(express))), "des_server_set_express")
         if order_min_points is not None:
             _check(self._L.des_server_set_order_min_points(h, int(order_min_points)),
                    "des_server_set_order_min_points")

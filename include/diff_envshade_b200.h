@@ -234,10 +234,6 @@ int des_server_set_order_min_points(des_server* s, int64_t n);
  * request without them, or least remaining work first (enable = 0).  Applies to requests admitted
  * after the call. */
 int des_server_set_rank_by_size(des_server* s, int enable);
-/* Express ticks on or off (default off): while every normal tick is queued on the GPU, requests
- * with at most six ticks of work left go whole into an extra tick (two at most at a time) on a
- * stream of the highest priority, which starts as soon as the running tick's CTAs finish. */
-int des_server_set_express(des_server* s, int enable);
 int des_server_stats(des_server* s, des_serve_stats* out);
 /* Finishes queued work and frees the server. */
 int des_server_destroy(des_server* s);
