@@ -132,26 +132,107 @@ struct TickCtl {
 // Batch kernel
 // ---------------------------------------------------------------------------------------------
 
+// Dynamic shared memory of the batch kernel: texel table [kMaxHWpad x 32 B], per-warp reduction
+// rows [kNW x 15 x 32 floats], then two buffers of prefetched tile points.
+constexpr size_t kSmemPts = (size_t)kMaxHWpad * 32 + (size_t)kNW * 15 * 32 * 4;
+
+// Asynchronous copies global -> shared (cp.async): 16 bytes bypassing L1, 4 bytes (zero-filled
+// when !ok, nothing read then), and the wait for all of the thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(__cvta_generic_to_global(gmem))
+               : "memory");
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool ok) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(__cvta_generic_to_global(gmem)),
+               "r"(ok ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The inputs of one tile's 32 consecutive points (a request in input order), copied into shared
+// memory with cp.async while the CTA computes the tile before it, so that the tile starts with its
+// points on chip (for inputs read in place from host memory, without a round trip over the host
+// link).  Entries past the request's last point are zero.
+struct TilePoints {
+  float normal[96], view[96], albedo[96], spec[96], gsh[96], gwh[96], bary[96], rough[32];
+  int64_t tri[32];
+};
+
+// A staged tile in the shape the point loader expects (index = lane, barycentric rows 32 apart).
+struct TileView {
+  const float* normal;
+  const float* view;
+  const int64_t* tri;
+  const float* bary;
+  int64_t P;
+  int N_face, N_vertex;
+  const int32_t* faces;
+  unsigned* ctrl;
+  bool clamp;
+};
+
+__device__ __forceinline__ TileView tile_view(const ReqDesc& r, const TilePoints* t) {
+  return TileView{t->normal, t->view, t->tri, t->bary, 32, r.N_face, r.N_vertex, r.faces, r.ctrl, r.clamp};
+}
+
+// Issues the copies of tile `tile` of request r (input order) into t: threads 0..127 copy 4-byte
+// words (a warp's copies cover whole 128-byte rows).  Completed by cp_async_wait_all.
+__device__ __forceinline__ void prefetch_points(const ReqDesc& r, int tile, bool adjoint, TilePoints* t) {
+  const int64_t first = (int64_t)tile * 32;
+  const int n = (int)min((int64_t)32, r.P - first);
+  const int i = threadIdx.x;
+  if (i < 96) {
+    const bool ok = i < 3 * n;
+    const int64_t o = ok ? 3 * first + i : 0;
+    cp_async4(&t->normal[i], r.normal + o, ok);
+    cp_async4(&t->view[i], r.view + o, ok);
+    cp_async4(&t->albedo[i], r.albedo + o, ok);
+    cp_async4(&t->spec[i], r.spec_alb + o, ok);
+    if (adjoint) {
+      cp_async4(&t->gsh[i], r.g_shading + o, ok);
+      if (r.g_white != nullptr) cp_async4(&t->gwh[i], r.g_white + o, ok);
+    }
+  } else if (i < 128) {
+    const int l = i - 96;
+    const bool ok = l < n;
+    const int64_t pid = ok ? first + l : 0;
+    cp_async4(&t->rough[l], r.rough + pid, ok);
+    if (r.has_vis) {
+      const float* tw = reinterpret_cast<const float*>(r.tri + pid);
+      float* td = reinterpret_cast<float*>(&t->tri[l]);
+      cp_async4(td, tw, ok);
+      cp_async4(td + 1, tw + 1, ok);
+      cp_async4(&t->bary[l], r.bary + pid, ok);
+      cp_async4(&t->bary[32 + l], r.bary + (ok ? pid + r.P : 0), ok);
+      cp_async4(&t->bary[64 + l], r.bary + (ok ? pid + 2 * r.P : 0), ok);
+    }
+  }
+}
+
 // The tiles run the shading kernels' per-pair arithmetic with the same point ordering, horizon
 // skip and mirrored texel split (des_shade.cu), so per-point results equal the plain path's
 // arithmetic for the same point and texel, whatever else shares the launch.
 template <bool DIFF, bool SPEC, bool VIS>
-__device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
+// pts: the tile's points already in shared memory (input order), or null to read them from r.
+__device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red, const TilePoints* pts) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t slot = (int64_t)tile * 32 + lane;
   int64_t pid = slot;
   const bool valid = ordered_point(r.perm, slot, r.P, r.ctrl, pid);
-  const PointGeom g = load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
+  const PointGeom g = pts ? load_geom<VIS>(tile_view(r, pts), lane, valid, SPEC || r.clamp)
+                          : load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
   SpecConst sc;
-  if (SPEC) sc = spec_const(valid ? r.rough[pid] : 0.f, g);
-  // the epilogue's albedos, fetched with the point (one round trip less for points read in place
-  // from host memory)
+  if (SPEC) sc = spec_const(valid ? (pts ? pts->rough[lane] : r.rough[pid]) : 0.f, g);
+  // the epilogue's albedos, fetched with the point
   float alb[3] = {0.f, 0.f, 0.f}, spa[3] = {0.f, 0.f, 0.f};
   if (warp == 0 && valid) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      if (DIFF) alb[c] = r.albedo[3 * pid + c];
-      if (SPEC) spa[c] = r.spec_alb[3 * pid + c];
+      if (DIFF) alb[c] = pts ? pts->albedo[3 * lane + c] : r.albedo[3 * pid + c];
+      if (SPEC) spa[c] = pts ? pts->spec[3 * lane + c] : r.spec_alb[3 * pid + c];
     }
   }
   float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -225,45 +306,53 @@ __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
 // texels in the same order (the pair weights are rounded in another association, so the outputs
 // equal a forward tile's within rounding).
 template <bool DIFF, bool SPEC>
-__device__ __forceinline__ void fwd_outputs(const ReqDesc& r, int64_t pid, bool valid, const float (&sums)[15],
+__device__ __forceinline__ void fwd_outputs(const float* alb, const float* spa, bool valid, const float (&sums)[15],
                                             float (&out)[3]) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     out[c] = 0.f;
-    if (DIFF) out[c] = (valid ? r.albedo[3 * pid + c] : 0.f) * sums[c];
-    if (SPEC) out[c] = fmaf(valid ? r.spec_alb[3 * pid + c] : 0.f, sums[3 + c], out[c]);
+    if (DIFF) out[c] = (valid ? alb[c] : 0.f) * sums[c];
+    if (SPEC) out[c] = fmaf(valid ? spa[c] : 0.f, sums[3 + c], out[c]);
   }
 }
 
 template <bool DIFF, bool SPEC, bool VIS>
-__device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
+// pts: the tile's points already in shared memory (input order), or null to read them from r.
+__device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red, const TilePoints* pts) {
   constexpr int NACC = 15;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t slot = (int64_t)tile * 32 + lane;
   int64_t pid = slot;
   const bool valid = ordered_point(r.perm, slot, r.P, r.ctrl, pid);
-  const PointGeom g = load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
+  const PointGeom g = pts ? load_geom<VIS>(tile_view(r, pts), lane, valid, SPEC || r.clamp)
+                          : load_geom<VIS>(r, pid, valid, SPEC || r.clamp);
+  // the point's own inputs: staged (index lane) or the request's arrays (index pid)
+  const int64_t ix = pts ? lane : pid;
+  const float* in_gsh = pts ? pts->gsh : r.g_shading;
+  const float* in_gwh = pts ? pts->gwh : r.g_white;
+  const float* in_alb = pts ? pts->albedo : r.albedo;
+  const float* in_spa = pts ? pts->spec : r.spec_alb;
   float gd0 = 0.f, gd1 = 0.f, gd2 = 0.f, gs0 = 0.f, gs1 = 0.f, gs2 = 0.f;
   if (valid) {
-    const float g0 = r.g_shading[3 * pid], g1 = r.g_shading[3 * pid + 1], g2 = r.g_shading[3 * pid + 2];
+    const float g0 = in_gsh[3 * ix], g1 = in_gsh[3 * ix + 1], g2 = in_gsh[3 * ix + 2];
     if (DIFF) {
-      gd0 = g0 * r.albedo[3 * pid];
-      gd1 = g1 * r.albedo[3 * pid + 1];
-      gd2 = g2 * r.albedo[3 * pid + 2];
+      gd0 = g0 * in_alb[3 * ix];
+      gd1 = g1 * in_alb[3 * ix + 1];
+      gd2 = g2 * in_alb[3 * ix + 2];
       if (r.g_white != nullptr) {
-        gd0 += r.g_white[3 * pid];
-        gd1 += r.g_white[3 * pid + 1];
-        gd2 += r.g_white[3 * pid + 2];
+        gd0 += in_gwh[3 * ix];
+        gd1 += in_gwh[3 * ix + 1];
+        gd2 += in_gwh[3 * ix + 2];
       }
     }
     if (SPEC) {
-      gs0 = g0 * r.spec_alb[3 * pid];
-      gs1 = g1 * r.spec_alb[3 * pid + 1];
-      gs2 = g2 * r.spec_alb[3 * pid + 2];
+      gs0 = g0 * in_spa[3 * ix];
+      gs1 = g1 * in_spa[3 * ix + 1];
+      gs2 = g2 * in_spa[3 * ix + 2];
     }
   }
   SpecConst sc;
-  if (SPEC) sc = spec_const(valid ? r.rough[pid] : 0.f, g);
+  if (SPEC) sc = spec_const(valid ? (pts ? pts->rough[lane] : r.rough[pid]) : 0.f, g);
   const BwdPoint gp{gd0, gd1, gd2, gs0, gs1, gs2};
   BwdAcc acc = {};
   const int nsl = r.HWpad >> 5;
@@ -330,13 +419,13 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
 #pragma unroll
       for (int q = 0; q < NACC; ++q) sums[q] += s_red[w * NACC * 32 + q * 32 + lane];
     if (r.perm == nullptr) {  // consecutive points: whole-row stores (outputs may be in host memory)
-      const float rough = (SPEC && valid) ? r.rough[pid] : 0.f;
-      const float g0 = valid ? r.g_shading[3 * pid] : 0.f, g1 = valid ? r.g_shading[3 * pid + 1] : 0.f,
-                  g2 = valid ? r.g_shading[3 * pid + 2] : 0.f;
+      const float rough = (SPEC && valid) ? (pts ? pts->rough[lane] : r.rough[pid]) : 0.f;
+      const float g0 = valid ? in_gsh[3 * ix] : 0.f, g1 = valid ? in_gsh[3 * ix + 1] : 0.f,
+                  g2 = valid ? in_gsh[3 * ix + 2] : 0.f;
       const BwdGrads q = bwd_point_grads<DIFF, SPEC>(sums, g, sc, rough, g0, g1, g2);
       const int64_t first = (int64_t)tile * 32;
       float out[3];
-      fwd_outputs<DIFF, SPEC>(r, pid, valid, sums, out);
+      fwd_outputs<DIFF, SPEC>(in_alb + 3 * ix, in_spa + 3 * ix, valid, sums, out);
       store_rows3(r.shading, first, r.P, out[0], out[1], out[2], lane);
       if (r.white != nullptr) store_rows3(r.white, first, r.P, sums[0], sums[1], sums[2], lane);
       store_rows3(r.g_normal, first, r.P, q.n[0], q.n[1], q.n[2], lane);
@@ -346,7 +435,7 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
       if (r.g_rough != nullptr && valid) r.g_rough[pid] = q.rough;
     } else if (valid) {
       float out[3];
-      fwd_outputs<DIFF, SPEC>(r, pid, valid, sums, out);
+      fwd_outputs<DIFF, SPEC>(in_alb + 3 * ix, in_spa + 3 * ix, valid, sums, out);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         r.shading[3 * pid + c] = out[c];
@@ -359,13 +448,14 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
 }
 
 template <bool FWD>
-__device__ __forceinline__ void dispatch_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red) {
+__device__ __forceinline__ void dispatch_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red,
+                                              const TilePoints* pts) {
   const int key = (r.diff ? 4 : 0) | (r.spec ? 2 : 0) | (r.has_vis ? 1 : 0);
   switch (key) {
 #define DES_TILE_CASE(K, D, S, V)                                       \
   case K:                                                               \
-    if (FWD) fwd_tile<D, S, V>(r, tile, s_tab, s_red);                  \
-    else bwd_tile<D, S, V>(r, tile, s_tab, s_red);                      \
+    if (FWD) fwd_tile<D, S, V>(r, tile, s_tab, s_red, pts);             \
+    else bwd_tile<D, S, V>(r, tile, s_tab, s_red, pts);                 \
     break;
     DES_TILE_CASE(7, true, true, true)
     DES_TILE_CASE(6, true, true, false)
@@ -383,16 +473,6 @@ __device__ __forceinline__ void dispatch_tile(const ReqDesc& r, int tile, const 
 // first tick that names the slot; a CTA copies the descriptor of the request it works on into
 // shared memory (one read over the host link per change of request).  slot_tiles: per slot, the
 // adjoint tiles finished so far over all of the slot's requests (never reset).
-// 16-byte asynchronous copy global -> shared (cp.async, bypassing L1), and the wait for all of the
-// thread's copies.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(__cvta_generic_to_global(gmem))
-               : "memory");
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
 __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __restrict__ reqs,
                                                             const WorkList* __restrict__ wl, TickCtl* ctl,
                                                             unsigned* __restrict__ slot_tiles,
@@ -400,40 +480,49 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* s_tab = reinterpret_cast<float4*>(smem_raw);
   float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)kMaxHWpad * 32);
+  TilePoints* s_pts = reinterpret_cast<TilePoints*>(smem_raw + kSmemPts);  // two buffers
   __shared__ __align__(16) ReqDesc s_desc;
-  __shared__ int s_idx[2];
-  __shared__ __align__(16) WorkItem s_item[2];
+  __shared__ int s_idx[3];
+  __shared__ __align__(16) WorkItem s_item[3];
+  __shared__ int s_pf_req[2], s_pf_tile[2], s_pf_kind[2];  // what each point buffer holds (req -1: nothing)
   __shared__ int s_last;
   const unsigned n = wl->n;
   int staged_req = -1;
   const float4* staged_table = nullptr;
-  // Thread 0 claims item indices one iteration ahead and copies the next item into shared memory
-  // with cp.async while the CTA works on the current one, so the read over the host link (the
-  // work list is mapped host memory) is off the tile's path; it waits for the copy just before
-  // the barrier that ends the iteration.
+  // Work items go through a ring of three: while the CTA computes item `it`, item it+1 is already
+  // in shared memory (its points are being prefetched), and thread 0 copies item it+2 in with
+  // cp.async (the work list is mapped host memory) and claims the index after it.  Every thread
+  // waits for its own copies just before the barrier that ends the iteration.
   int claimed = 0;
   if (threadIdx.x == 0) {
-    const int i0 = (int)atomicAdd(&ctl->next, 1u);
-    s_idx[0] = i0;
-    if (i0 < (int)n) s_item[0] = wl->items[i0];
+    for (int j = 0; j < 2; ++j) {
+      const int i0 = (int)atomicAdd(&ctl->next, 1u);
+      s_idx[j] = i0;
+      if (i0 < (int)n) s_item[j] = wl->items[i0];
+      s_pf_req[j] = -1;
+    }
     claimed = (int)atomicAdd(&ctl->next, 1u);
   }
   __syncthreads();
   for (int it = 0;; ++it) {
-    const int idx = s_idx[it & 1];
+    const int idx = s_idx[it % 3];
     if (idx >= (int)n) break;
-    const WorkItem item = s_item[it & 1];
+    const WorkItem item = s_item[it % 3];
+    const bool has_next = s_idx[(it + 1) % 3] < (int)n;
+    const WorkItem next = s_item[(it + 1) % 3];
+    const int pb = it & 1;  // point buffer of this item; the next item's is pb ^ 1
+    const bool pre = s_pf_req[pb] == item.req && s_pf_tile[pb] == item.tile && s_pf_kind[pb] == item.kind;
+    __syncthreads();  // everyone has read the ring and the buffer tags before thread 0 rewrites them
     if (threadIdx.x == 0) {
-      s_idx[(it + 1) & 1] = claimed;
-      if (claimed < (int)n) cp_async16(&s_item[(it + 1) & 1], &wl->items[claimed]);
+      s_idx[(it + 2) % 3] = claimed;
+      if (claimed < (int)n) cp_async16(&s_item[(it + 2) % 3], &wl->items[claimed]);
       claimed = (int)atomicAdd(&ctl->next, 1u);
+      s_pf_req[pb ^ 1] = -1;
     }
     // a malformed work item is reported and skipped, never dereferenced
     if (item.req < 0 || item.req >= kMaxSlots || (item.kind != 0 && item.kind != 1) || item.tile < 0) {
-      if (threadIdx.x == 0) {
-        atomicOr(&ctrl[kCtrlError], 4u);
-        cp_async_wait_all();
-      }
+      if (threadIdx.x == 0) atomicOr(&ctrl[kCtrlError], 4u);
+      cp_async_wait_all();
       __syncthreads();
       continue;
     }
@@ -455,17 +544,26 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
     }
     const ReqDesc& r = s_desc;
     if ((int64_t)item.tile * 32 >= r.P) {
-      if (threadIdx.x == 0) {
-        atomicOr(&ctrl[kCtrlError], 4u);
-        cp_async_wait_all();
-      }
+      if (threadIdx.x == 0) atomicOr(&ctrl[kCtrlError], 4u);
+      cp_async_wait_all();
       __syncthreads();
       continue;
     }
+    // the next item continues this request in input order: copy its points in while this one runs
+    if (has_next && next.req == item.req && r.perm == nullptr && (next.kind == 0 || next.kind == 1) &&
+        next.tile >= 0 && (int64_t)next.tile * 32 < r.P) {
+      prefetch_points(r, next.tile, next.kind == 1, &s_pts[pb ^ 1]);
+      if (threadIdx.x == 0) {
+        s_pf_req[pb ^ 1] = next.req;
+        s_pf_tile[pb ^ 1] = next.tile;
+        s_pf_kind[pb ^ 1] = next.kind;
+      }
+    }
+    const TilePoints* pts = pre ? &s_pts[pb] : nullptr;
     if (item.kind == 0) {
-      dispatch_tile<true>(r, item.tile, s_tab, s_red);
+      dispatch_tile<true>(r, item.tile, s_tab, s_red, pts);
     } else {
-      dispatch_tile<false>(r, item.tile, s_tab, s_red);
+      dispatch_tile<false>(r, item.tile, s_tab, s_red, pts);
       // the CTA that finishes a request's last adjoint tile converts its FP64 env gradient and
       // leaves the accumulator zeroed for its next user
       __syncthreads();
@@ -483,7 +581,7 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
         }
       }
     }
-    if (threadIdx.x == 0) cp_async_wait_all();
+    cp_async_wait_all();
     __syncthreads();
   }
   // every CTA has made its last claim before it counts itself out; the last one resets the tick
@@ -735,7 +833,7 @@ struct des_server {
   int device = 0;
   int tick_us = 150;
   double pairs_per_us = 0;  // the batch kernel's throughput, which sizes the ticks
-  std::atomic<int> ticks_in_flight{3};  // tick buffers in use at once (<= kNTicks)
+  std::atomic<int> ticks_in_flight{4};  // tick buffers in use at once (<= kNTicks)
   std::atomic<int64_t> order_min_p{des::serve::kServeOrderMinP};  // requests with fewer points are shaded in input order
   des::serve::CopyLane up, down;
   des::serve::OrderLane order;
@@ -1377,7 +1475,7 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
     return DES_ERR_CUDA;
   }
   for (int i = des::serve::kMaxSlots - 1; i >= 0; --i) s->free_slots.push_back(i);
-  s->smem = (size_t)des::serve::kMaxHWpad * 32 + (size_t)des::serve::kNW * 15 * 32 * 4;
+  s->smem = des::serve::kSmemPts + 2 * sizeof(des::serve::TilePoints);
   if (cudaFuncSetAttribute(des::serve::batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem) !=
       cudaSuccess) {
     des_server_destroy(s);

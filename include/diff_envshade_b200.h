@@ -222,7 +222,7 @@ int des_server_submit(des_server* s, const des_serve_request* req, int64_t* tick
 int des_server_poll(des_server* s, des_serve_done* out, int max_items, int* count);
 /* Waits until every submitted request has finished (DES_ERR_TIMEOUT after timeout_ms). */
 int des_server_drain(des_server* s, int timeout_ms);
-/* How many ticks may be queued on the GPU at once (1..4, default 3): more overlaps consecutive
+/* How many ticks may be queued on the GPU at once (1..4, default 4): more overlaps consecutive
  * ticks better, fewer lets a newly arrived request start sooner. */
 int des_server_set_ticks_in_flight(des_server* s, int n);
 /* Requests of at least n points (and at least 16384) are ordered by normal direction before they
