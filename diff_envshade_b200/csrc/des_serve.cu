@@ -4,17 +4,18 @@
 // scheduler thread
 //   * admits them in arrival order while a device arena of fixed size (the HBM budget) has room,
 //     skipping over requests that do not fit yet, and uploads their point data through a copy lane
-//     that sends the least remaining work first, in slices (downloads use a second lane); requests
-//     shaded in input order whose buffers the device can reach (its own memory, pinned host
-//     memory) skip the copies: the batch kernel reads their inputs and stores their outputs in
-//     place;
+//     that sends the lowest-ranked request first, in slices (downloads use a second lane);
+//     requests shaded in input order whose buffers the device can reach (its own memory, pinned
+//     host memory) skip the copies: the batch kernel reads their inputs and stores their outputs
+//     in place;
 //   * keeps env maps (their texel tables) and meshes (faces + visibility words) resident, shared by
 //     reference between requests;
-//   * every tick packs 32-point tiles of the admitted requests into a work list, smallest
-//     remaining work first, up to a time budget, into a work list in mapped pinned memory and
+//   * every tick packs 32-point tiles of the ready requests, lowest rank first (remaining points x
+//     texels, or remaining work), up to a time budget, into a work list in mapped pinned memory and
 //     launches it as a CUDA graph (one persistent batch kernel) on its own stream, with up to
 //     ticks_in_flight ticks queued so that consecutive ticks overlap;
-//   * when every tile of a request has finished, copies its outputs back and frees its memory.
+//   * when every tile of a request has finished, copies its outputs back (unless they were stored
+//     in place) and frees its memory.
 // Work of different requests therefore shares each launch and each SM; a request that arrives
 // while others run joins the next tick.
 //
@@ -72,7 +73,9 @@ constexpr int64_t kServeOrderMinP = INT64_MAX;
 // Throughput of the batch kernel on a 148-SM B200 in pair units per microsecond (a forward pair is
 // one unit, an adjoint pair two), measured on mixed workloads; it converts tick_us into work.  A
 // fixed figure: an estimate taken from the ticks themselves feeds back on itself (under-filled
-// ticks leave SMs idle, which lowers the estimate, which shrinks the ticks).
+// ticks leave SMs idle, which lowers the estimate, which shrinks the ticks).  (A per-tile cost model
+// fitted to single-request ticks made the mixed workload's ticks smaller and lost throughput
+// without shortening the tail.)
 constexpr double kBatchPairsPerUs = 3.5e5;
 
 // Device-side request descriptor (member names shared with ShadeParams for the point loaders).
@@ -670,7 +673,8 @@ struct Req {
   int slot = -1;
   int n_tiles = 0;
   int fwd_issued = 0, bwd_issued = 0, fwd_done = 0, bwd_done = 0;
-  double cost_fwd_tile = 0, cost_bwd_tile = 0;
+  double cost_fwd_tile = 0, cost_bwd_tile = 0;  // pair units per tile
+  double tile_pairs = 0;                         // point x texel pairs per tile
   ReqDesc desc{};
   int32_t* d_perm = nullptr;         // normal-direction order (see orders()), else null
   int64_t order_min_p = 0;           // the server's ordering threshold when the request was admitted
@@ -698,13 +702,13 @@ struct Req {
   double rank() const {
     if (!rank_by_size) return remaining();
     const int left = in.backward ? n_tiles - std::min(fwd_issued, bwd_issued) : n_tiles - fwd_issued;
-    return left * cost_fwd_tile;
+    return left * tile_pairs;
   }
 };
 
 // Host<->device copies of the requests go through two copy lanes (one stream per direction, so
 // uploads and downloads overlap).  A request's copies form a job of segments; a lane issues its jobs
-// in slices, always from the job with the lowest priority value (least remaining work for uploads,
+// in slices, always from the job with the lowest priority value (the request's rank for uploads,
 // fewest bytes for downloads), and keeps a bounded number of bytes queued on its stream.  A small
 // request therefore waits for at most about one queue's worth of a large one's transfer instead
 // of all of it.  (Copies of one direction share a copy engine in submission order, so a short
@@ -720,7 +724,7 @@ struct CopyJob {
   std::vector<CopySeg> segs;
   size_t seg = 0, seg_off = 0;  // next byte to issue
   int outstanding = 0;          // issued slices not yet complete
-  double prio = 0;              // lower goes first: the request's work (uploads), bytes (downloads)
+  double prio = 0;              // lower goes first: the request's rank (uploads), bytes (downloads)
   bool issued_all() const { return seg >= segs.size(); }
   void add(void* dst, const void* src, size_t bytes) {
     if (bytes) segs.push_back(CopySeg{dst, src, bytes});
@@ -825,7 +829,6 @@ struct Mesh {
 };
 
 struct Tick {
-  double units = 0;       // work packed into the tick (pair units)
   WorkList* h = nullptr;  // pinned, mapped
   WorkList* d = nullptr;  // the device's address of h
   TickCtl* ctl = nullptr;
@@ -842,8 +845,8 @@ struct Tick {
 struct des_server {
   int device = 0;
   int tick_us = 150;
-  double pairs_per_us = 0;  // the batch kernel's throughput, which sizes the ticks
   std::atomic<int> ticks_in_flight{4};  // tick buffers in use at once (<= kNTicks)
+  double pairs_per_us = 0;              // the batch kernel's throughput, which sizes the ticks
   std::atomic<int64_t> order_min_p{des::serve::kServeOrderMinP};  // requests with fewer points are shaded in input order
   des::serve::CopyLane up, down;
   des::serve::OrderLane order;
@@ -1225,7 +1228,7 @@ bool launch_tick(des_server* s) {
   }
   if (t == nullptr || busy >= s->ticks_in_flight) return false;
   const double budget = s->pairs_per_us * s->tick_us;
-  // shortest remaining work first, ties by arrival (the set's order); at least one item per
+  // lowest rank first, ties by arrival (the set's order); at least one item per
   // resident CTA while there is work, so that no SM idles for want of items
   double used = 0;
   unsigned n = 0;
@@ -1251,7 +1254,6 @@ bool launch_tick(des_server* s) {
     t->counts.push_back({r, {nf, nb}});
     if (r->remaining() > 0) s->ready.insert({r->rank(), r->ticket, r});  // budget is used up
   }
-  t->units = used;
   t->h->n = n;
   std::atomic_thread_fence(std::memory_order_seq_cst);  // items are in host memory before the launch
   if (cudaGraphLaunch(t->exec, t->stream) != cudaSuccess) {
@@ -1334,9 +1336,9 @@ void worker_loop(des_server* s) {
       r->n_tiles = (int)((r->in.P + 31) / 32);
       // a request with gradients runs adjoint tiles only: they store its forward outputs too
       if (r->in.backward) r->fwd_issued = r->fwd_done = r->n_tiles;
-      const double pairs = 32.0 * E.HWpad;
-      r->cost_fwd_tile = pairs;
-      r->cost_bwd_tile = 2.0 * pairs;
+      r->tile_pairs = 32.0 * E.HWpad;
+      r->cost_fwd_tile = r->tile_pairs;
+      r->cost_bwd_tile = 2.0 * r->tile_pairs;
       s->active.insert(r);
       if (upload(s, r)) {
         r->state = State::Uploading;
@@ -1462,7 +1464,6 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
     return DES_ERR_CUDA;
   }
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
-  // a conservative starting throughput; it only sizes ticks
   s->pairs_per_us = des::serve::kBatchPairsPerUs * s->sms / 148.0;
   bool ok = s->up.init(cudaMemcpyHostToDevice, size_t(1) << 20, size_t(4) << 20) &&
             s->down.init(cudaMemcpyDeviceToHost, size_t(1) << 20, size_t(4) << 20) && s->order.init() &&
