@@ -61,6 +61,7 @@ constexpr int kMaxHWpad = 2048;      // texel table kept in shared memory per CT
 constexpr int kMaxSlots = 8192;      // concurrently admitted requests
 constexpr int kTickItems = 4096;     // work items per tick (upper bound; the whole list is uploaded)
 constexpr int kNTicks = 4;           // tick buffers (up to this many ticks in flight)
+constexpr int kQueuedTicks = 1;      // launched ticks not yet started by the GPU, at most
 constexpr int kCopyEvents = 64;                    // completion events per copy lane
 // Default ordering threshold of the server (requests of at least this many points are ordered by
 // normal direction): none.  An ordered request must be uploaded (the ordering kernels and the
@@ -121,7 +122,9 @@ struct WorkItem {
 // (mapped), so a tick needs no host-to-device copy: the batch kernel fetches each item over the
 // host link while it computes the previous one.
 struct WorkList {
-  unsigned n, pad0, pad1, pad2;
+  unsigned n;        // items in the list (written by the scheduler)
+  unsigned started;  // set to 1 by the CTA that claims item 0 (the tick is running)
+  unsigned pad0, pad1;
   WorkItem items[kTickItems];
 };
 
@@ -484,10 +487,12 @@ __device__ __forceinline__ void dispatch_tile(const ReqDesc& r, int tile, const 
 
 // reqs: the slots' descriptors in mapped pinned host memory, written by the scheduler before the
 // first tick that names the slot; a CTA copies the descriptor of the request it works on into
-// shared memory (one read over the host link per change of request).  slot_tiles: per slot, the
-// adjoint tiles finished so far over all of the slot's requests (never reset).
+// shared memory (one read over the host link per change of request).  started: the work list's
+// flag that the CTA claiming item 0 sets (mapped; the scheduler reads it).  slot_tiles: per slot,
+// the adjoint tiles finished so far over all of the slot's requests (never reset).
 __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __restrict__ reqs,
-                                                            const WorkList* __restrict__ wl, TickCtl* ctl,
+                                                            const WorkList* __restrict__ wl,
+                                                            unsigned* started, TickCtl* ctl,
                                                             unsigned* __restrict__ slot_tiles,
                                                             unsigned* __restrict__ ctrl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -511,6 +516,7 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
     for (int j = 0; j < 2; ++j) {
       const int i0 = (int)atomicAdd(&ctl->next, 1u);
       s_idx[j] = i0;
+      if (i0 == 0) *reinterpret_cast<volatile unsigned*>(started) = 1u;  // tells the scheduler
       if (i0 < (int)n) s_item[j] = wl->items[i0];
       s_pf_req[j] = -1;
     }
@@ -863,7 +869,7 @@ struct des_server {
   std::vector<des::serve::Env> envs;
   std::vector<des::serve::Mesh> meshes;
   des::serve::Tick ticks[des::serve::kNTicks];
-  std::atomic<bool> rank_by_size{true};
+  std::atomic<bool> rank_by_size{false};
   int sms = 0, grid = 0;
   size_t smem = 0;
 
@@ -1227,6 +1233,13 @@ bool launch_tick(des_server* s) {
       t = &k;
   }
   if (t == nullptr || busy >= s->ticks_in_flight) return false;
+  // at most kQueuedTicks launched ticks that no CTA has started yet: the next one is launched as
+  // soon as the GPU begins the last queued one, which keeps the SMs fed across tick boundaries
+  // while a request that becomes ready waits behind little queued work
+  int queued = 0;
+  for (auto& k : s->ticks)
+    if (k.busy && *reinterpret_cast<volatile unsigned*>(&k.h->started) == 0u) ++queued;
+  if (queued >= kQueuedTicks) return false;
   const double budget = s->pairs_per_us * s->tick_us;
   // lowest rank first, ties by arrival (the set's order); at least one item per
   // resident CTA while there is work, so that no SM idles for want of items
@@ -1255,11 +1268,13 @@ bool launch_tick(des_server* s) {
     if (r->remaining() > 0) s->ready.insert({r->rank(), r->ticket, r});  // budget is used up
   }
   t->h->n = n;
+  t->h->started = 0u;
   std::atomic_thread_fence(std::memory_order_seq_cst);  // items are in host memory before the launch
   if (cudaGraphLaunch(t->exec, t->stream) != cudaSuccess) {
     // launch the same work without the graph
     cudaGetLastError();
-    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_desc, t->d, t->ctl, s->d_slot_tiles, s->d_ctrl);
+    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_desc, t->d, &t->d->started, t->ctl,
+                                                            s->d_slot_tiles, s->d_ctrl);
     s->stats.device_error |= 16;
   }
   count_launches(1);
@@ -1511,8 +1526,8 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
     std::memset(t.h, 0, sizeof(des::serve::WorkList));
     cudaGraph_t g = nullptr;
     ok = cudaStreamBeginCapture(t.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    des::serve::batch_kernel<<<s->grid, des::serve::kNW * 32, s->smem, t.stream>>>(s->d_desc, t.d, t.ctl,
-                                                                                   s->d_slot_tiles, s->d_ctrl);
+    des::serve::batch_kernel<<<s->grid, des::serve::kNW * 32, s->smem, t.stream>>>(
+        s->d_desc, t.d, &t.d->started, t.ctl, s->d_slot_tiles, s->d_ctrl);
     ok = ok && cudaStreamEndCapture(t.stream, &g) == cudaSuccess;
     ok = ok && cudaGraphInstantiate(&t.exec, g, 0) == cudaSuccess;
     if (g) cudaGraphDestroy(g);
