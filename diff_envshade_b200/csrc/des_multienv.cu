@@ -10,14 +10,16 @@
 // each tile accumulates hi*hi + lo*hi + hi*lo in FP32 (error ~2^-16 relative).  DES_RELIGHT_BF16
 // keeps only hi*hi (plain BF16 inputs, error ~2^-8 relative per term).
 //
-// Kernel structure (one persistent CTA per SM, 14 warps):
-//   warps 0-7   builders: per 32-texel stage, 128 points x 32 texels of A_c (3 channels, hi and lo)
+// Kernel structure (one persistent CTA per SM, 22 warps):
+//   warps 0-15  builders: per 32-texel stage, 128 points x 32 texels of A_c (3 channels, hi and lo)
 //               written to shared memory in the UMMA K-major no-swizzle canonical layout
-//               (8-row x 16-byte core matrices, 128 B each);
-//   warp 8      allocates 512 TMEM columns; lane 0 issues tcgen05.mma (M=128, N=Kpad, K=16) and
+//               (8-row x 16-byte core matrices, 128 B each); four threads per point row, one
+//               8-texel chunk each (sixteen warps hide the latency of the weight build better
+//               than eight: the build, not the MMA, bounds the kernel);
+//   warp 16     allocates 512 TMEM columns; lane 0 issues tcgen05.mma (M=128, N=Kpad, K=16) and
 //               tcgen05.commit to the stage-empty / accumulator-full mbarriers;
-//   warps 9-12  epilogue: tcgen05.ld of the finished tile (32 TMEM lanes per warp) -> global;
-//   warp 13     lane 0 streams the prepared BF16 radiance tile of each stage with cp.async.bulk
+//   warps 17-20 epilogue: tcgen05.ld of the finished tile (32 TMEM lanes per warp) -> global;
+//   warp 21     lane 0 streams the prepared BF16 radiance tile of each stage with cp.async.bulk
 //               (a plain bulk copy from this GPU's memory; no multicast).
 // Two shared-memory stages and two TMEM accumulator buffers (2 x 3 x Kpad columns) let the weight
 // build, the MMAs and the epilogue overlap.  Every mbarrier wait is bounded (2 s of %globaltimer):
@@ -42,11 +44,11 @@ constexpr int kTileM = 128;                  // points per tile (UMMA M)
 constexpr int kStageT = 32;                  // texels per stage (one visibility slot)
 constexpr int kNStage = 2;                   // shared-memory ring depth
 constexpr int kEnvBlock = 64;                // env maps per pass
-constexpr int kBuilderThreads = 256;         // warps 0-7
-constexpr int kCtrlWarp = 8;
-constexpr int kEpiWarp0 = 9;                 // warps 9-12
-constexpr int kProdWarp = 13;
-constexpr int kThreads = 14 * 32;
+constexpr int kBuilderThreads = 512;         // warps 0-15
+constexpr int kCtrlWarp = 16;
+constexpr int kEpiWarp0 = 17;                // warps 17-20
+constexpr int kProdWarp = 21;
+constexpr int kThreads = 22 * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr int kATile = kTileM * kStageT * 2;  // bytes of one BF16 [128 x 32] operand tile
 constexpr long long kWaitNs = 2000000000LL;
@@ -266,7 +268,8 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
 
   if (threadIdx.x < kBuilderThreads) {
     // ------------------------------------------------------------------ weight builders
-    const int row = threadIdx.x & 127, half = threadIdx.x >> 7;
+    // four builder threads per point row, each building one 8-texel chunk of every stage
+    const int row = threadIdx.x & 127, quarter = threadIdx.x >> 7;
     const bool need_view = SPEC || p.pt.clamp;
     uint32_t q = 0;
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
@@ -290,25 +293,24 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
         const uint32_t b = q & 1u, u = q >> 1;
         uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
         if (VIS) {
-          w0 = n0 >> (16 * half);
-          w1 = n1 >> (16 * half);
-          w2 = n2 >> (16 * half);
+          w0 = n0 >> (8 * quarter);
+          w1 = n1 >> (8 * quarter);
+          w2 = n2 >> (8 * quarter);
           if (st + 1 < p.nst) load_vis_words(p.pt, g, valid, st + 1, n0, n1, n2);
         }
         // the whole warp leaves together (the texel votes below need all 32 lanes)
         if (u > 0 && !__all_sync(0xffffffffu, mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err))) goto builders_done;
         {
           const uint32_t abuf = a_base + b * (3 * 2 * kATile);
-#pragma unroll
-          for (int j8 = 0; j8 < 2; ++j8) {
+          {
             uint32_t hi[3][4], lo[3][4];
 #pragma unroll
             for (int jj = 0; jj < 8; jj += 2) {
               float av[3][2];
 #pragma unroll
               for (int e = 0; e < 2; ++e) {
-                const int jl = j8 * 8 + jj + e;  // 0..15 within this thread's half stage
-                const int t = st * kStageT + half * 16 + jl;
+                const int jl = jj + e;  // 0..7 within this thread's chunk
+                const int t = st * kStageT + quarter * 8 + jl;
                 const float4 A = s_tab[2 * t];
                 // texel below the horizon of the warp's 32 (ordered) points: zero weights
                 if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) {
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
 #pragma unroll
               for (int c = 0; c < 3; ++c) split2(av[c][0], av[c][1], hi[c][jj / 2], lo[c][jj / 2]);
             }
-            const int kc = half * 2 + j8;  // 8-texel chunk within the stage
+            const int kc = quarter;  // 8-texel chunk within the stage
             const uint32_t off = (uint32_t)(((row >> 3) * 4 + kc) * 128 + (row & 7) * 16);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
