@@ -244,17 +244,12 @@ __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
   float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   const int nsl = r.HWpad >> 5;
   const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
-  // visibility words of the next slot are loaded while this one is integrated (as in the plain
-  // kernels): the gather otherwise stalls every slot
-  uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
-  int sl = warp_slot(0, warp, kNW, nsl, ushift);
-  if (VIS && sl >= 0) load_vis_words(r, g, valid, sl, n0, n1, n2);
-  for (int k = 1; sl >= 0; ++k) {
-    const int cur = sl;
-    sl = warp_slot(k, warp, kNW, nsl, ushift);
-    uint32_t w0 = n0, w1 = n1, w2 = n2;
+  for (int k = 0;; ++k) {
+    const int cur = warp_slot(k, warp, kNW, nsl, ushift);
+    if (cur < 0) break;
+    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
     if (VIS) {
-      if (sl >= 0) load_vis_words(r, g, valid, sl, n0, n1, n2);
+      load_vis_words(r, g, valid, cur, w0, w1, w2);
       if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
     }
     const float4* rec = s_tab + 2 * (cur << 5);
@@ -369,17 +364,12 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
   const int nsl = r.HWpad >> 5;
   const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
   const int jsel = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-  // visibility words of the next slot are loaded while this one is integrated (as in the plain
-  // kernels): the gather otherwise stalls every slot
-  uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
-  int sl = warp_slot(0, warp, kNW, nsl, ushift);
-  if (VIS && sl >= 0) load_vis_words(r, g, valid, sl, n0, n1, n2);
-  for (int k = 1; sl >= 0; ++k) {
-    const int cur = sl;
-    sl = warp_slot(k, warp, kNW, nsl, ushift);
-    uint32_t w0 = n0, w1 = n1, w2 = n2;
+  for (int k = 0;; ++k) {
+    const int cur = warp_slot(k, warp, kNW, nsl, ushift);
+    if (cur < 0) break;
+    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
     if (VIS) {
-      if (sl >= 0) load_vis_words(r, g, valid, sl, n0, n1, n2);
+      load_vis_words(r, g, valid, cur, w0, w1, w2);
       if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
     }
     const float4* rec = s_tab + 2 * (cur << 5);

@@ -229,6 +229,41 @@ def run(n=2000, rate=5000.0, tick_us=75, serial=True, hbm_budget_bytes=40 << 30,
     return res
 
 
+def run_single(P, vis=False, backward=False, reps=2, H=16, W=32, tick_us=75, seed=4242):
+    """One request shape submitted `reps` times, one after the other, to an otherwise idle server
+    (inputs and outputs in pinned host memory, so it is read and written in place): each one's
+    compute time (ready -> last tile done, ms) and the ticks it took.  For timing and profiling the
+    batch kernel on a single kind of tile."""
+    from .serving import Server
+    g = torch.Generator().manual_seed(seed)
+    inp = wl.make_inputs(P, 4, 8, seed=seed)
+    pin = {k: getattr(inp, k).pin_memory() for k in ("normal", "view_dir", "albedo", "specular_albedo", "roughness",
+                                                      "grad_shading", "grad_diffuse_shading")}
+    kw = {}
+    with Server(device=0, hbm_budget_bytes=4 << 30, tick_us=tick_us) as srv:
+        env_id = srv.add_envmap(torch.exp(torch.randn(3, H, W, generator=g)))
+        if vis:
+            faces = torch.randint(0, 100000, (3, 200000), generator=g).to(torch.int32)
+            bits = wl.pack_bits(torch.rand(100000, (H * W + 31) // 32 * 32, generator=g) < 0.7)
+            e = -torch.log(torch.rand(3, P, generator=g).clamp_min(1e-12))
+            kw = dict(mesh_id=srv.add_mesh(faces, bits),
+                      nearest_triangle_id=torch.randint(0, 200000, (P,), generator=g).pin_memory(),
+                      barycentric_coord=(e / e.sum(0, keepdim=True)).contiguous().pin_memory())
+        times = []
+        for _ in range(reps):
+            r = srv.submit(pin["normal"], pin["view_dir"], pin["albedo"], pin["specular_albedo"], pin["roughness"],
+                           env_id=env_id, backward=backward, grad_shading=pin["grad_shading"],
+                           grad_diffuse_shading=pin["grad_diffuse_shading"], **kw)
+            srv.drain(60)
+            srv.poll()
+            if r.status != 0:
+                raise RuntimeError(f"request failed (status {r.status})")
+            times.append((r.stages["computed"] - r.stages["ready"]) * 1e-6)
+        st = srv.stats()
+    return {"points": P, "texels": H * W, "visibility": vis, "backward": backward, "compute_ms": times,
+            "ticks": st["ticks"], "device_error": st["device_error"]}
+
+
 if __name__ == "__main__":
     import argparse
     import json
@@ -238,6 +273,13 @@ if __name__ == "__main__":
     ap.add_argument("--tick-us", type=int, default=75)
     ap.add_argument("--ticks-in-flight", type=int, default=None)
     ap.add_argument("--no-serial", action="store_true")
+    ap.add_argument("--single", type=int, default=0, help="time one request of this many points instead")
+    ap.add_argument("--vis", action="store_true", help="(--single) with visibility")
+    ap.add_argument("--backward", action="store_true", help="(--single) with gradients")
+    ap.add_argument("--reps", type=int, default=2, help="(--single) submissions, one after the other")
     a = ap.parse_args()
-    print(json.dumps(run(n=a.n, rate=a.rate, tick_us=a.tick_us, serial=not a.no_serial,
-                         ticks_in_flight=a.ticks_in_flight)))
+    if a.single > 0:
+        print(json.dumps(run_single(a.single, vis=a.vis, backward=a.backward, reps=a.reps, tick_us=a.tick_us)))
+    else:
+        print(json.dumps(run(n=a.n, rate=a.rate, tick_us=a.tick_us, serial=not a.no_serial,
+                             ticks_in_flight=a.ticks_in_flight)))
