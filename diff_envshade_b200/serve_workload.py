@@ -229,18 +229,23 @@ def run(n=2000, rate=5000.0, tick_us=75, serial=True, hbm_budget_bytes=40 << 30,
     return res
 
 
-def run_single(P, vis=False, backward=False, reps=2, H=16, W=32, tick_us=75, seed=4242):
-    """One request shape submitted `reps` times, one after the other, to an otherwise idle server
-    (inputs and outputs in pinned host memory, so it is read and written in place): each one's
-    compute time (ready -> last tile done, ms) and the ticks it took.  For timing and profiling the
-    batch kernel on a single kind of tile."""
+def run_single(P, vis=False, backward=False, reps=2, H=16, W=32, tick_us=75, seed=4242, where="host",
+               order_min_points=None):
+    """One request shape submitted `reps` times, one after the other, to an otherwise idle server:
+    each one's compute time (ready -> last tile done, ms) and the ticks it took.  For timing and
+    profiling the batch kernel on a single kind of tile.  where="host": inputs and outputs in
+    pinned host memory (read and written in place over the host link); "device": inputs in device
+    memory (read in place, no host link).  order_min_points: the server's ordering threshold (an
+    ordered request is uploaded first)."""
     from .serving import Server
     g = torch.Generator().manual_seed(seed)
     inp = wl.make_inputs(P, 4, 8, seed=seed)
     pin = {k: getattr(inp, k).pin_memory() for k in ("normal", "view_dir", "albedo", "specular_albedo", "roughness",
                                                       "grad_shading", "grad_diffuse_shading")}
+    if where == "device":
+        pin = {k: v.cuda() for k, v in pin.items()}
     kw = {}
-    with Server(device=0, hbm_budget_bytes=4 << 30, tick_us=tick_us) as srv:
+    with Server(device=0, hbm_budget_bytes=4 << 30, tick_us=tick_us, order_min_points=order_min_points) as srv:
         env_id = srv.add_envmap(torch.exp(torch.randn(3, H, W, generator=g)))
         if vis:
             faces = torch.randint(0, 100000, (3, 200000), generator=g).to(torch.int32)
@@ -249,6 +254,9 @@ def run_single(P, vis=False, backward=False, reps=2, H=16, W=32, tick_us=75, see
             kw = dict(mesh_id=srv.add_mesh(faces, bits),
                       nearest_triangle_id=torch.randint(0, 200000, (P,), generator=g).pin_memory(),
                       barycentric_coord=(e / e.sum(0, keepdim=True)).contiguous().pin_memory())
+            if where == "device":
+                kw["nearest_triangle_id"] = kw["nearest_triangle_id"].cuda()
+                kw["barycentric_coord"] = kw["barycentric_coord"].cuda()
         times = []
         for _ in range(reps):
             r = srv.submit(pin["normal"], pin["view_dir"], pin["albedo"], pin["specular_albedo"], pin["roughness"],
@@ -260,8 +268,9 @@ def run_single(P, vis=False, backward=False, reps=2, H=16, W=32, tick_us=75, see
                 raise RuntimeError(f"request failed (status {r.status})")
             times.append((r.stages["computed"] - r.stages["ready"]) * 1e-6)
         st = srv.stats()
-    return {"points": P, "texels": H * W, "visibility": vis, "backward": backward, "compute_ms": times,
-            "ticks": st["ticks"], "device_error": st["device_error"]}
+    return {"points": P, "texels": H * W, "visibility": vis, "backward": backward, "inputs": where,
+            "order_min_points": order_min_points, "compute_ms": times, "ticks": st["ticks"],
+            "device_error": st["device_error"]}
 
 
 if __name__ == "__main__":
@@ -277,9 +286,13 @@ if __name__ == "__main__":
     ap.add_argument("--vis", action="store_true", help="(--single) with visibility")
     ap.add_argument("--backward", action="store_true", help="(--single) with gradients")
     ap.add_argument("--reps", type=int, default=2, help="(--single) submissions, one after the other")
+    ap.add_argument("--device-inputs", action="store_true", help="(--single) inputs in device memory")
+    ap.add_argument("--order-min-points", type=int, default=None, help="(--single) the ordering threshold")
     a = ap.parse_args()
     if a.single > 0:
-        print(json.dumps(run_single(a.single, vis=a.vis, backward=a.backward, reps=a.reps, tick_us=a.tick_us)))
+        print(json.dumps(run_single(a.single, vis=a.vis, backward=a.backward, reps=a.reps, tick_us=a.tick_us,
+                                    where="device" if a.device_inputs else "host",
+                                    order_min_points=a.order_min_points)))
     else:
         print(json.dumps(run(n=a.n, rate=a.rate, tick_us=a.tick_us, serial=not a.no_serial,
                              ticks_in_flight=a.ticks_in_flight)))
