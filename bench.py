@@ -424,6 +424,7 @@ def main():
         e2e = {"value": world * P * HW / (e2e_ms / K * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / K,
                "serial_ms_per_step": serial_ms / K,
+               "l2": "not flushed between steps: every step's inputs arrive afresh over the host link",
                "api": "diff_envshade_b200.shade + torch.autograd.backward (every step uploads all of its "
                       "inputs from one pinned host block and downloads every output into pinned host "
                       "memory; step i+1's upload and step i's download overlap compute on two copy "
