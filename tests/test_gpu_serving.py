@@ -196,3 +196,40 @@ def test_outputs_in_place_and_staged_agree():
     for key, got in results.items():
         _compare(got, ref, f"{key}", exact=True)
         assert_close_grad(got["g_envmap"], ref["g_envmap"], f"{key}:g_envmap")
+
+
+def test_requests_may_omit_outputs():
+    """A request may leave outputs out (no diffuse shading, no view or roughness gradient): the
+    outputs it names equal those of the same request naming all of them, whether they are stored
+    in place (pinned host) or staged (pageable host), and nothing else is written."""
+    from diff_envshade_b200.serving import Server
+    g = torch.Generator().manual_seed(31)
+    faces, vis_bits = _mesh(13)
+    env = torch.exp(torch.randn(3, 16, 32, generator=g))
+    inp, tri, bary = _points(9001, seed=90, N_face=faces.shape[1])
+    keep = ("shading", "g_normal", "g_albedo", "g_specular_albedo", "g_envmap")
+    with Server(device=0, hbm_budget_bytes=1 << 30, tick_us=100) as srv:
+        env_id = srv.add_envmap(env)
+        mesh_id = srv.add_mesh(faces, vis_bits)
+
+        def run(outs):
+            req = srv.submit(inp.normal, inp.view_dir, inp.albedo, inp.specular_albedo, inp.roughness,
+                             env_id=env_id, mesh_id=mesh_id, nearest_triangle_id=tri, barycentric_coord=bary,
+                             backward=True, grad_shading=inp.grad_shading,
+                             grad_diffuse_shading=inp.grad_diffuse_shading, outputs=outs)
+            srv.drain(60)
+            srv.poll()
+            assert req.status == 0
+            return {k: v.clone() for k, v in outs.items()}
+
+        full = run(_outputs(inp.P, 16, 32, "pinned"))
+        for where in ("pinned", "pageable"):
+            some = {k: v for k, v in _outputs(inp.P, 16, 32, where).items() if k in keep}
+            got = run(some)
+            assert set(got) == set(keep)
+            for k in keep:
+                if k == "g_envmap":
+                    assert_close_grad(got[k], full[k], f"{where}:{k}")
+                else:
+                    assert torch.equal(got[k], full[k]), f"{where}:{k} differs"
+        assert srv.stats()["device_error"] == 0
