@@ -1211,6 +1211,23 @@ void finish_request(des_server* s, Req* r, int64_t t_done) {
   delete r;
 }
 
+// Reports a request that was never admitted (no slot, arena range or accumulator) as finished with
+// the given error status.
+void reject_request(des_server* s, Req* r, int status) {
+  des_serve_done d{};
+  d.ticket = r->ticket;
+  d.t_submit_ns = r->t_submit - s->t0;
+  d.t_done_ns = now_ns() - s->t0;
+  d.status = status;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->completed.push_back(d);
+    s->n_done += 1;
+  }
+  s->cv.notify_all();
+  delete r;
+}
+
 // Builds and launches one tick if a tick buffer is free.  Returns true when work was launched.
 bool launch_tick(des_server* s) {
   if (s->ready.empty()) return false;
@@ -1321,6 +1338,13 @@ void worker_loop(des_server* s) {
       r->rank_by_size = s->rank_by_size.load();
       resolve_request(s, r);
       r->bytes = request_layout(r->in, E, r->order_min_p, r->inplace_in, nullptr).bytes;
+      if ((r->bytes + 255) / 256 * 256 > s->arena.total()) {
+        // can never fit: finish it now with an error instead of letting it wait for memory forever
+        reject_request(s, r, DES_ERR_WORKSPACE);
+        it = s->pending.erase(it);
+        progressed = true;
+        continue;
+      }
       size_t off = 0;
       if (r->in.backward && s->acc_pool.empty() && !grow_acc_pool(s)) {
         ++it;

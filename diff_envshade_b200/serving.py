@@ -151,6 +151,8 @@ class Server:
         tensors to write into (pinned or pageable host tensors, or CUDA tensors on the server's
         device).  Inputs and outputs must stay untouched until the request is done."""
         P = normal.shape[0]
+        if env_id not in self._envs:
+            _check(1, f"submit: unknown env_id {env_id}")  # DES_ERR_INVALID_ARGUMENT, as the C ABI returns
         H, W = self._envs[env_id]
         dv = self._device
         ins = {k: _host(v, torch.float32, dv) for k, v in (("normal", normal), ("view_dir", view_dir),

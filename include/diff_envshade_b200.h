@@ -208,8 +208,10 @@ int des_server_add_envmap(des_server* s, int32_t H, int32_t W, const float* envm
 /* Registers a resident mesh: faces (3 x N_face) and visibility words (N_slot x N_vertex). */
 int des_server_add_mesh(des_server* s, int32_t N_face, int32_t N_vertex, int32_t N_slot,
                         const int32_t* face_vertex_list, const int32_t* visibility, int32_t* mesh_id);
-/* Queues a request; returns immediately with its ticket.  After a CUDA error the server fails every
- * outstanding request (status DES_ERR_CUDA in des_serve_done) and refuses new ones.  When every
+/* Queues a request; returns immediately with its ticket (DES_ERR_INVALID_ARGUMENT, and no ticket,
+ * for a malformed request).  A request whose buffers could never fit the HBM budget finishes at
+ * once with status DES_ERR_WORKSPACE.  After a CUDA error the server fails every outstanding
+ * request (status DES_ERR_CUDA in des_serve_done) and refuses new ones.  When every
  * output the request names is device memory of the server's device, or pinned host memory and the
  * request is shaded in input order, the batch kernel stores the results there directly; otherwise
  * they are staged in the arena and copied back.  Either way they are in place when the request is

@@ -233,3 +233,42 @@ def test_requests_may_omit_outputs():
                 else:
                     assert torch.equal(got[k], full[k]), f"{where}:{k} differs"
         assert srv.stats()["device_error"] == 0
+
+
+
+def test_malformed_and_oversized_requests():
+    """Malformed requests are refused at submission -- an unknown env map or mesh, a mesh with too
+    few visibility slots for the env map, no shading term -- and leave the server working; a
+    request whose buffers could never fit the HBM budget finishes at once with DES_ERR_WORKSPACE
+    (3) instead of waiting for memory forever."""
+    import ctypes
+    from diff_envshade_b200 import workloads as wl
+    from diff_envshade_b200.serving import Server, _Request
+    g = torch.Generator().manual_seed(41)
+    faces16, vis16 = _mesh(14, n_slots=16)  # 512 visibility bits: enough for 16x32, not for 32x64
+    inp, tri, bary = _points(1000, seed=41, N_face=faces16.shape[1])
+    with Server(device=0, hbm_budget_bytes=8 << 20, tick_us=100) as srv:
+        e16 = srv.add_envmap(torch.exp(torch.randn(3, 16, 32, generator=g)))
+        e32 = srv.add_envmap(torch.exp(torch.randn(3, 32, 64, generator=g)))
+        mesh = srv.add_mesh(faces16, vis16)
+        for env_id, mesh_id in ((99, -1), (e16, 7), (e32, mesh)):
+            with pytest.raises(RuntimeError):
+                _submit(srv, inp, tri, bary, env_id, mesh_id, False)
+        good = _submit(srv, inp, tri, bary, e16, mesh, False)
+        # no shading term (flags 0), through the C ABI
+        q = _Request()
+        q.P, q.env_id, q.mesh_id, q.flags, q.backward = inp.P, e16, -1, 0, 0
+        for k in ("normal", "view_dir", "albedo", "specular_albedo", "roughness"):
+            setattr(q, k, good._inputs[k].data_ptr())
+        q.shading = good.outputs["shading"].data_ptr()
+        ticket = ctypes.c_int64()
+        assert srv._L.des_server_submit(srv._h, ctypes.byref(q), ctypes.byref(ticket)) == 1
+        # the outputs of 500k points alone take 12 MB of arena: more than the 8 MiB budget
+        big = wl.make_inputs(500000, 4, 8, seed=42)
+        huge = srv.submit(big.normal, big.view_dir, big.albedo, big.specular_albedo, big.roughness, env_id=e16)
+        after = _submit(srv, inp, tri, bary, e16, mesh, True)
+        srv.drain(60)
+        srv.poll()
+        assert good.status == 0 and after.status == 0
+        assert huge.status == 3
+        assert srv.stats()["device_error"] == 0
