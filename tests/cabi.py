@@ -1,7 +1,7 @@
 """ctypes view of the C ABI (include/diff_envshade_b200.h) used by the tests.
 
-This is the binding a C-ABI consumer would write (INTEGRATION.md shows the same stub); the
-tests call the library through it directly, without the torch extension.
+This is the binding a C-ABI consumer written in Python would use (plain ctypes over the shared
+library); the tests call the library through it directly, without the torch extension.
 """
 import ctypes
 import os
