@@ -47,6 +47,9 @@ def _relight(des, d, envs, vis, split):
     (777, 16, 32, 70, True, True),     # two passes (64 + 6 env maps), ragged point count
     (513, 8, 16, 24, False, True),
     (1000, 16, 32, 16, True, False),   # plain BF16
+    (1, 16, 32, 1, True, True),        # one point, one env map
+    (300, 32, 64, 8, True, True),      # the largest map the kernel takes (2048 texels)
+    (129, 16, 16, 3, False, False),    # 256 texels, ragged points, plain BF16
 ])
 def test_relight_against_fp64_oracle(P, H, W, K, vis, split):
     import diff_envshade_b200 as des
