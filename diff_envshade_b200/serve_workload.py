@@ -85,6 +85,9 @@ def prepare_barycentrics(pools, sched):
 
 
 def _summarize(lat_s, sched, makespan_s):
+    """p50/p99/mean/max latency (ms) over all requests and over the 50k-100k-point 16x32 class, and
+    throughput: requests per second and point x texel pairs per second, a request with gradients
+    counting its pairs twice (forward and adjoint pass)."""
     lat = np.asarray(lat_s) * 1e3
     pairs = sum(r["P"] * r["res"][0] * r["res"][1] * (2 if r["backward"] else 1) for r in sched)
     cls = [i for i, r in enumerate(sched) if 50000 <= r["P"] <= 100000 and r["res"] == (16, 32)]
