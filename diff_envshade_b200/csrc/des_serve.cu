@@ -840,7 +840,7 @@ struct Tick {
 
 struct des_server {
   int device = 0;
-  int tick_us = 150;
+  int tick_us = 75;
   std::atomic<int> ticks_in_flight{4};  // tick buffers in use at once (<= kNTicks)
   double pairs_per_us = 0;              // the batch kernel's throughput, which sizes the ticks
   std::atomic<int64_t> order_min_p{des::serve::kServeOrderMinP};  // requests with fewer points are shaded in input order
