@@ -171,12 +171,34 @@ def cpu_port_throughput(inp, target_s=8.0, max_points=None):
     return total_pairs / total_t, desc, threads
 
 
+def load_workloads():
+    """The seeded input generators (diff_envshade_b200/workloads.py, which needs only numpy and
+    torch), loaded from their file so that the package -- and with it the native extension -- is
+    not imported: the reference arm maps no library of this build."""
+    import importlib.util
+    path = os.path.join(ROOT, "diff_envshade_b200", "workloads.py")
+    spec = importlib.util.spec_from_file_location("_des_bench_workloads", path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses resolve the module by name
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def bench_config(P, H, W, nbits, world):
+    """The `config` object of both arms' JSON lines (one definition, so they always agree)."""
+    return {"workload": f"{CONFIG_NAME}: {P} points x {H}x{W} env, {nbits}-bit visibility, specular on, fwd+bwd",
+            "points_per_rank": P, "texels": H * W, "parallelism": f"dp{world}" if world > 1 else "single",
+            "l2": "256 MiB buffer rewritten between timed steps (outside the timed events)"}
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    from diff_envshade_b200 import workloads as wl
-    inp = wl.make_config(CONFIG_NAME)
+    wl = load_workloads()
+    c = wl.CONFIGS[CONFIG_NAME]
+    # rank 0's inputs of the GPU arm (same seed, same draws)
+    inp = wl.make_inputs(c["P"], c["H"], c["W"], c["seed"], sigma=c["sigma"], rough=c["rough"], vis_p=c["vis_p"])
     # each step is a bounded sample; the whole arm stays within about two minutes
     per_step_s = min(2.0, max(0.05, 120.0 / max(args.steps + args.warmup, 1)))
     vals = []
@@ -190,10 +212,12 @@ def run_reference_arm(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": pairs / value * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": f"{CONFIG_NAME}: 70000 points x 16x32 env, 512-bit visibility, specular on",
-                   "note": "reference has no CPU path: C++ FP32 restatement of its sum (oracle port)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded normals/views/materials, lognormal env, Bernoulli(0.7) bits)",
+        "config": bench_config(inp.P, c["H"], c["W"], inp.visibility.shape[0] * 32, args.gpus),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": desc + "; the reference has no CPU path: C++ FP32 restatement of its sum "
+                                          "(oracle port), each step a bounded sample of the workload's points"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -472,10 +496,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded normals/views/materials, lognormal env, Bernoulli(0.7) bits)",
-            "config": {"workload": f"{CONFIG_NAME}: {P} points x {d.envmap.shape[1]}x{d.envmap.shape[2]} env, "
-                                   f"{d.visibility.shape[0] * 32}-bit visibility, specular on, fwd+bwd",
-                       "points_per_rank": P, "texels": HW, "parallelism": f"dp{world}" if world > 1 else "single",
-                       "l2": "256 MiB buffer rewritten between timed steps (outside the timed events)"},
+            "config": bench_config(P, d.envmap.shape[1], d.envmap.shape[2], d.visibility.shape[0] * 32, world),
             "gpu_launches": launches,
             "roofline": roofline,
             "cpu_baseline": cpu,

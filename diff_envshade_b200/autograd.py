@@ -5,8 +5,13 @@ these Functions are the wrapping a caller of the reference would write: ``forwar
 ``*_forward*`` operator and saves its inputs, ``backward`` calls the matching ``*_backward*``
 operator with the incoming gradients (zeros for an output that received none).  Light rotation,
 mesh indices, barycentrics and visibility receive no gradient, as in the reference.
+
+The backward operators are native kernels that autograd cannot trace, so every ``backward`` is
+``once_differentiable``: asking for second derivatives (``create_graph=True``) raises instead of
+silently returning zeros.
 """
 import torch
+from torch.autograd.function import once_differentiable
 
 from . import _C
 
@@ -25,6 +30,7 @@ class DiffuseShade(torch.autograd.Function):
         return shading
 
     @staticmethod
+    @once_differentiable
     def backward(ctx, g_shading):
         normal, albedo, envmap, rot = ctx.saved_tensors
         gn, ga, ge = _C.bruteforce_diffuse_shader_backward(_grad_or_zeros(g_shading, albedo), normal, albedo,
@@ -63,6 +69,7 @@ class SpecularShade(_SpecularV1):
                                       light2obj_rotmat, enable_diffuse, enable_specular)
 
     @staticmethod
+    @once_differentiable
     def backward(ctx, g_shading):
         return SpecularShade._backward(ctx, g_shading)
 
@@ -82,6 +89,7 @@ class SpecularShadeClamp(_SpecularV1):
                                            light2obj_rotmat, enable_diffuse, enable_specular)
 
     @staticmethod
+    @once_differentiable
     def backward(ctx, g_shading):
         return SpecularShadeClamp._backward(ctx, g_shading)
 
@@ -105,6 +113,7 @@ class SpecularShade2(torch.autograd.Function):
         return shading, white
 
     @staticmethod
+    @once_differentiable
     def backward(ctx, g_shading, g_white):
         normal, view, albedo, spec, rough, envmap, rot = ctx.saved_tensors
         gn, gv, ga, gs, gr, ge = _C.bruteforce_specular_shader_backward2(
@@ -129,6 +138,7 @@ class SpecularVisibilityShade2(torch.autograd.Function):
         return shading, white
 
     @staticmethod
+    @once_differentiable
     def backward(ctx, g_shading, g_white):
         (normal, view, albedo, spec, rough, envmap, rot, faces, tri, bary, vis) = ctx.saved_tensors
         gn, gv, ga, gs, gr, ge = _C.bruteforce_specularvisibility_shader_backward2(

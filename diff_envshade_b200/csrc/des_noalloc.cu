@@ -19,6 +19,12 @@
 //    the tile counter and error word and overwrites the texel table and every env-gradient partial it
 //    reads, so nothing left over is ever used -- but two calls whose work overlaps on the GPU (other
 //    streams, other host threads) race on the array and corrupt each other's results;
+//  * DES_REUSE_ORDER is ignored here: no forward ever leaves its point ordering in this array, so a
+//    call that ordered its points always computes the ordering itself (a permutation left over from
+//    an earlier call of another size would drop points);
+//  * errors found on the device (out-of-range triangle or vertex ids, which des_workspace_status
+//    reports for a caller-owned workspace) are not observable through this entry point: such points
+//    shade to zero, as with the regular entry point, but the error word is not handed to the caller;
 //  * the first call on each device looks up the array's device address with cudaGetSymbolAddress
 //    (once per device, with that device current); that first call should be made before any CUDA
 //    stream capture is started.
@@ -61,6 +67,7 @@ extern "C" int des_shade_backward_noalloc(const des_shade_args* args, unsigned f
                                           float* g_albedo, float* g_specular_albedo, float* g_roughness,
                                           float* g_envmap, des_stream_t stream) {
   if (args == nullptr) return DES_ERR_INVALID_ARGUMENT;
+  flags &= ~(unsigned)DES_REUSE_ORDER;  // the array never holds a forward's ordering
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return DES_ERR_CUDA;
   const size_t need = des_shade_workspace_bytes(args->P, args->H, args->W, flags | DES_COMPACT, 1, dev);

@@ -127,7 +127,9 @@ int des_shade_backward(const des_shade_args* args, unsigned flags, const float* 
  * (a problem that fits only a smaller plan runs with that plan, see DES_COMPACT).  All calls share the
  * array: calls whose work overlaps on the GPU race and corrupt each other.  The first call on each
  * device looks up the array's address (cudaGetSymbolAddress); make it before any stream capture.
- * Allocates nothing. */
+ * DES_REUSE_ORDER is ignored (the array never holds a forward's ordering).  Out-of-range mesh ids
+ * found on the device shade to zero but are not reported (there is no caller-visible workspace for
+ * des_workspace_status to read).  Allocates nothing. */
 int des_shade_backward_noalloc(const des_shade_args* args, unsigned flags, const float* grad_shading,
                                const float* grad_diffuse_shading, float* g_normal, float* g_view_dir,
                                float* g_albedo, float* g_specular_albedo, float* g_roughness, float* g_envmap,

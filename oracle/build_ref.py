@@ -11,6 +11,9 @@ what a stock ``TORCH_CUDA_ARCH_LIST=10.0`` build of that setup.py would pass, so
 kernels are the reference's default-flag (no fast-math, ``-fmad=true``) code.
 
 Usage:  python oracle/build_ref.py [--src /path/to/reference] [-j N]
+The source directory is ``--src``, else the environment variable ``DES_REFERENCE_SRC``; with
+neither, or when the directory holds no ``bruteforce_shader.cu``, nothing is built and the script
+exits 0 (the GPU tests that need the reference then skip).
 Outputs go only to ``oracle/_ref/`` (git-ignored; it travels with the repo snapshot).
 """
 import argparse
@@ -35,13 +38,16 @@ def _torch_paths():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--src", default=os.environ.get("DES_REFERENCE_SRC"))
     ap.add_argument("-j", type=int, default=3)
     args = ap.parse_args()
+    if not args.src:
+        print("no reference source directory (--src or DES_REFERENCE_SRC); nothing built")
+        return 0
     src = os.path.abspath(args.src)
     if not os.path.isfile(os.path.join(src, "bruteforce_shader.cu")):
         print(f"reference sources not found under {src}; nothing built")
-        return 1
+        return 0
     os.makedirs(OUT, exist_ok=True)
     inc, lib, abi = _torch_paths()
     py_inc = sysconfig.get_paths()["include"]

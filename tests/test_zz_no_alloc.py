@@ -73,6 +73,53 @@ def test_noalloc_backward_matches_workspace_entry_point_twice():
             assert_close_grad(g.cpu(), w.cpu(), f"noalloc:{name}")
 
 
+SCRATCH = 4 << 20  # DES_SHADE_NOALLOC_SCRATCH_BYTES
+
+
+def _plan_bytes(L, P, H, W, flags):
+    return L.des_shade_workspace_bytes(P, H, W, flags, 1, torch.cuda.current_device())
+
+
+def test_noalloc_ordered_plan_ignores_reuse_flag():
+    """A small map whose ordered plan fits the array (8x8 texels, 20,000 points: the points are
+    ordered by normal direction inside the array).  DES_REUSE_ORDER is passed on purpose: no forward
+    ever left an ordering in the array, so the entry point must order the points itself -- twice in
+    a row with different point counts, so a stale permutation would lose points the second time."""
+    from diff_envshade_b200 import workloads as wl
+    L = _lib()
+    flags = cabi.DES_DIFFUSE | cabi.DES_SPECULAR
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for P, seed in ((20000, 811), (17000, 812)):
+        assert _plan_bytes(L, P, 8, 8, flags) <= SCRATCH  # the default (ordered) plan fits
+        d = wl.make_inputs(P, 8, 8, seed=seed, vis_p=0.7, vis_layout="mesh", rotation=True).to("cuda")
+        args = cabi.make_args(d)
+        want = _with_workspace(L, args, flags, d, stream)
+        got = _noalloc(L, args, flags | cabi.DES_REUSE_ORDER, d, stream)
+        torch.cuda.synchronize()
+        for name, g, w in zip(GRAD_NAMES, got, want):
+            assert_close_grad(g.cpu(), w.cpu(), f"noalloc-ordered:{name}")
+
+
+def test_noalloc_input_order_fallback():
+    """Sizes whose ordered plan does not fit the array but whose input-order plan does (8x16 texels,
+    300,000 points on a 148-SM B200): the call shades in input order with the default CTA width."""
+    from diff_envshade_b200 import workloads as wl
+    L = _lib()
+    flags = cabi.DES_DIFFUSE | cabi.DES_SPECULAR
+    P, H, W = 300000, 8, 16
+    ordered, unordered = _plan_bytes(L, P, H, W, flags), _plan_bytes(L, P, H, W, flags | cabi.DES_INPUT_ORDER)
+    if not (ordered > SCRATCH >= unordered):
+        pytest.skip(f"plan sizes on this device do not isolate the input-order fallback ({ordered}, {unordered})")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    d = wl.make_inputs(P, H, W, seed=821, vis_p=0.6, vis_layout="identity", rotation=True).to("cuda")
+    args = cabi.make_args(d)
+    want = _with_workspace(L, args, flags, d, stream)
+    got = _noalloc(L, args, flags, d, stream)
+    torch.cuda.synchronize()
+    for name, g, w in zip(GRAD_NAMES, got, want):
+        assert_close_grad(g.cpu(), w.cpu(), f"noalloc-input-order:{name}")
+
+
 def test_noalloc_refuses_problems_larger_than_its_scratch():
     L = _lib()
     flags = cabi.DES_DIFFUSE | cabi.DES_SPECULAR
