@@ -9,7 +9,7 @@ Each product is rebuilt only when one of its sources is newer than it.  The comp
 keep nvcc's defaults for floating point (-fmad=true, IEEE division, no fast-math), which the
 bit-exact texel table depends on.
 
-Usage:  python -m diff_envshade_b200.build [--force] [--verbose]
+Usage:  python diff_envshade_b200/build.py [--force] [--verbose] [--ptxas]
 """
 import argparse
 import glob

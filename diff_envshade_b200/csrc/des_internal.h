@@ -100,6 +100,8 @@ int launch_texel_table(int H, int W, const float* R, float* out, des_stream_t st
 int launch_table(int H, int W, int HWpad, const float* R, const float* env, float4* rec, unsigned* ctrl,
                  cudaStream_t stream);
 void set_timing_events(cudaEvent_t start, cudaEvent_t stop);
+// The events set by set_timing_events (both null when timing is off).
+void timing_events(cudaEvent_t& start, cudaEvent_t& stop);
 // Normal-direction ordering of P points on its own (kSortMinP..kSortMaxP points): perm[P] receives
 // the point indices in the order the shading kernels use; scratch needs point_order_scratch_bytes(P).
 size_t point_order_scratch_bytes(int64_t P);

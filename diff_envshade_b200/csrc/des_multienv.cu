@@ -214,10 +214,81 @@ __global__ void prep_kernel(const float* __restrict__ env, int HW, int nst, int 
   *reinterpret_cast<__nv_bfloat16*>(base + tile + canon_off(k, j)) = lo;
 }
 
+// ---- weight builders -----------------------------------------------------------------------
+
+// One builder thread's share of one tile: for every 32-texel stage, the 8-texel chunk `quarter` of
+// point row `row` -- A_c = albedo_c wd + specular_c ws for c = 0..2, as BF16 hi and lo parts -- into
+// the stage's shared-memory A tiles (K-major canonical layout).  Texels are taken in pairs: a pair
+// below the horizon of the warp's 32 (ordered) points gets zero weights after one vote, otherwise
+// both are evaluated side by side.  The visibility words of the next stage are loaded while this one
+// is built.  q counts the stages this thread has filled (ring position).  Returns false when the CTA
+// gave up waiting (the whole warp leaves together).
+template <bool DIFF, bool SPEC, bool VIS, bool ONEV>
+__device__ __forceinline__ bool build_tile(const Params& p, const float4* s_tab, const PointGeom& g, bool valid,
+                                           const SpecConst& sc, const float (&alb)[3], const float (&spc)[3], int row,
+                                           int quarter, uint32_t& q, uint32_t a_base, uint64_t* full_a,
+                                           uint64_t* empty, volatile int* s_abort, unsigned* err) {
+  const float cs = (g.c0 + g.c1) + g.c2;
+  uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
+  if (VIS) load_vis_words<ONEV>(p.pt, g, valid, 0, n0, n1, n2);
+  for (int st = 0; st < p.nst; ++st, ++q) {
+    const uint32_t b = q & 1u, u = q >> 1;
+    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
+    if (VIS) {
+      w0 = n0 >> (8 * quarter);
+      w1 = n1 >> (8 * quarter);
+      w2 = n2 >> (8 * quarter);
+      if (st + 1 < p.nst) load_vis_words<ONEV>(p.pt, g, valid, st + 1, n0, n1, n2);
+    }
+    // the whole warp leaves together (the texel votes below need all 32 lanes)
+    if (u > 0 && !__all_sync(0xffffffffu, mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err))) return false;
+    const uint32_t abuf = a_base + b * (3 * 2 * kATile);
+    uint32_t hi[3][4], lo[3][4];
+#pragma unroll
+    for (int jj = 0; jj < 8; jj += 2) {
+      const int t = st * kStageT + quarter * 8 + jj;
+      const float4 A0 = s_tab[2 * t];
+      const float4 A1 = s_tab[2 * t + 2];
+      const float nl0 = dot3(g.nx, g.ny, g.nz, A0.x, A0.y, A0.z);
+      const float nl1 = dot3(g.nx, g.ny, g.nz, A1.x, A1.y, A1.z);
+      if (!__any_sync(0xffffffffu, nl0 > 0.f || nl1 > 0.f)) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) hi[c][jj / 2] = lo[c][jj / 2] = 0u;
+        continue;
+      }
+      const float4 B0 = s_tab[2 * t + 1];
+      const float4 B1 = s_tab[2 * t + 3];
+      const float vis0 = pair_vis<VIS, ONEV>(w0, w1, w2, 1u << jj, g, cs);
+      const float vis1 = pair_vis<VIS, ONEV>(w0, w1, w2, 2u << jj, g, cs);
+      float wd0, ws0, wd1, ws1;
+      pair_fwd_weights<DIFF, SPEC>(g, sc, A0, B0.w, nl0, vis0, wd0, ws0);
+      pair_fwd_weights<DIFF, SPEC>(g, sc, A1, B1.w, nl1, vis1, wd1, ws1);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        split2(fmaf(alb[c], wd0, spc[c] * ws0), fmaf(alb[c], wd1, spc[c] * ws1), hi[c][jj / 2], lo[c][jj / 2]);
+    }
+    const uint32_t off = (uint32_t)(((row >> 3) * 4 + quarter) * 128 + (row & 7) * 16);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const uint32_t ahi = abuf + (uint32_t)(c * 2) * kATile + off;
+      asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ahi), "r"(hi[c][0]), "r"(hi[c][1]), "r"(hi[c][2]),
+                   "r"(hi[c][3])
+                   : "memory");
+      if (p.split)
+        asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ahi + kATile), "r"(lo[c][0]), "r"(lo[c][1]),
+                     "r"(lo[c][2]), "r"(lo[c][3])
+                     : "memory");
+    }
+    fence_proxy_async_smem();
+    mbar_arrive(&full_a[b]);
+  }
+  return true;
+}
+
 // ---- main kernel ---------------------------------------------------------------------------
 
 template <bool DIFF, bool SPEC, bool VIS>
-__global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
+__global__ void __maxnreg__(88) relight_kernel(const Params p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int HWpad = p.pt.HWpad;
   const Smem L = smem_layout(HWpad, p.kpad);
@@ -286,68 +357,13 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
           if (SPEC) spc[c] = p.pt.spec[3 * pid + c];
         }
       }
-      // visibility words of the next stage are loaded while this one is built
-      uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
-      if (VIS) load_vis_words(p.pt, g, valid, 0, n0, n1, n2);
-      for (int st = 0; st < p.nst; ++st, ++q) {
-        const uint32_t b = q & 1u, u = q >> 1;
-        uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
-        if (VIS) {
-          w0 = n0 >> (8 * quarter);
-          w1 = n1 >> (8 * quarter);
-          w2 = n2 >> (8 * quarter);
-          if (st + 1 < p.nst) load_vis_words(p.pt, g, valid, st + 1, n0, n1, n2);
-        }
-        // the whole warp leaves together (the texel votes below need all 32 lanes)
-        if (u > 0 && !__all_sync(0xffffffffu, mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err))) goto builders_done;
-        {
-          const uint32_t abuf = a_base + b * (3 * 2 * kATile);
-          {
-            uint32_t hi[3][4], lo[3][4];
-#pragma unroll
-            for (int jj = 0; jj < 8; jj += 2) {
-              float av[3][2];
-#pragma unroll
-              for (int e = 0; e < 2; ++e) {
-                const int jl = jj + e;  // 0..7 within this thread's chunk
-                const int t = st * kStageT + quarter * 8 + jl;
-                const float4 A = s_tab[2 * t];
-                // texel below the horizon of the warp's 32 (ordered) points: zero weights
-                if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) {
-#pragma unroll
-                  for (int c = 0; c < 3; ++c) av[c][e] = 0.f;
-                  continue;
-                }
-                const float4 B = s_tab[2 * t + 1];
-                const float vis = VIS ? vis_weight(w0, w1, w2, 1u << jl, g.c0, g.c1, g.c2) : 1.f;
-                float wd, ws;
-                pair_fwd_weights<DIFF, SPEC>(g, sc, A, B.w, vis, wd, ws);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) av[c][e] = fmaf(alb[c], wd, spc[c] * ws);
-              }
-#pragma unroll
-              for (int c = 0; c < 3; ++c) split2(av[c][0], av[c][1], hi[c][jj / 2], lo[c][jj / 2]);
-            }
-            const int kc = quarter;  // 8-texel chunk within the stage
-            const uint32_t off = (uint32_t)(((row >> 3) * 4 + kc) * 128 + (row & 7) * 16);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              const uint32_t ahi = abuf + (uint32_t)(c * 2) * kATile + off;
-              asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ahi), "r"(hi[c][0]), "r"(hi[c][1]),
-                           "r"(hi[c][2]), "r"(hi[c][3])
-                           : "memory");
-              if (p.split)
-                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ahi + kATile), "r"(lo[c][0]),
-                             "r"(lo[c][1]), "r"(lo[c][2]), "r"(lo[c][3])
-                             : "memory");
-            }
-          }
-        }
-        fence_proxy_async_smem();
-        mbar_arrive(&full_a[b]);
-      }
+      const bool onev = VIS && warp_single_vertex(g);
+      const bool ok = onev ? build_tile<DIFF, SPEC, VIS, true>(p, s_tab, g, valid, sc, alb, spc, row, quarter, q,
+                                                               a_base, full_a, empty, s_abort, err)
+                           : build_tile<DIFF, SPEC, VIS, false>(p, s_tab, g, valid, sc, alb, spc, row, quarter, q,
+                                                                a_base, full_a, empty, s_abort, err);
+      if (!ok) break;
     }
-  builders_done:;
   } else if (warp == kCtrlWarp) {
     // ------------------------------------------------------------------ MMA issue (one thread)
     if (lane == 0) {
@@ -602,8 +618,13 @@ int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigne
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total) != cudaSuccess)
       return DES_ERR_CUDA;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    timing_events(ev0, ev1);
+    const bool timed = ev0 != nullptr && ev1 != nullptr && kbase == 0;  // the first pass of K
+    if (timed) cudaEventRecord(ev0, stream);
     k<<<grid, relight::kThreads, L.total, stream>>>(prm);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
+    if (timed) cudaEventRecord(ev1, stream);
     count_launches(2);
   }
   return DES_OK;

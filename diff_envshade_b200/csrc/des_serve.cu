@@ -221,6 +221,59 @@ __device__ __forceinline__ void prefetch_points(const ReqDesc& r, int tile, bool
 // The tiles run the shading kernels' per-pair arithmetic with the same point ordering, horizon
 // skip and mirrored texel split (des_shade.cu), so per-point results equal the plain path's
 // arithmetic for the same point and texel, whatever else shares the launch.
+
+// The kNW warps' share of a tile's texel slots (mirrored pairs); a slot whose visibility words are
+// zero for all 32 lanes is skipped.
+template <bool DIFF, bool SPEC, bool VIS, bool ONEV>
+__device__ __forceinline__ void fwd_tile_slots(const ReqDesc& r, const PointGeom& g, bool valid, const SpecConst& sc,
+                                               const float4* s_tab, float (&acc)[6]) {
+  const int warp = threadIdx.x >> 5;
+  const float cs = (g.c0 + g.c1) + g.c2;
+  const int nsl = r.HWpad >> 5;
+  const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
+  for (int k = 0;; ++k) {
+    const int cur = warp_slot(k, warp, kNW, nsl, ushift);
+    if (cur < 0) break;
+    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
+    if (VIS) {
+      load_vis_words<ONEV>(r, g, valid, cur, w0, w1, w2);
+      if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
+    }
+    fwd_slot<DIFF, SPEC, VIS, ONEV>(g, sc, cs, s_tab + 2 * (cur << 5), w0, w1, w2, acc);
+  }
+}
+
+// As fwd_tile_slots for the adjoint; each 8-texel group's env-map gradient is added to the
+// request's FP64 accumulator.
+template <bool DIFF, bool SPEC, bool VIS, bool ONEV>
+__device__ __forceinline__ void bwd_tile_slots(const ReqDesc& r, const PointGeom& g, bool valid, const SpecConst& sc,
+                                               const BwdPoint& gp, const float4* s_tab, BwdAcc& acc) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float cs = (g.c0 + g.c1) + g.c2;
+  const int nsl = r.HWpad >> 5;
+  const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
+  const int jsel = butterfly_texel(lane);
+  for (int k = 0;; ++k) {
+    const int cur = warp_slot(k, warp, kNW, nsl, ushift);
+    if (cur < 0) break;
+    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
+    if (VIS) {
+      load_vis_words<ONEV>(r, g, valid, cur, w0, w1, w2);
+      if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
+    }
+    const int t0 = (cur << 5) + jsel;
+    auto sink = [&](int gq, float y0, float y1, float y2) {
+      if ((lane & 3) == 0) {
+        const int t = t0 + gq * 8;
+        atomicAdd(r.env_acc + t, (double)y0);
+        atomicAdd(r.env_acc + r.HWpad + t, (double)y1);
+        atomicAdd(r.env_acc + 2 * r.HWpad + t, (double)y2);
+      }
+    };
+    bwd_slot<DIFF, SPEC, VIS, ONEV>(g, sc, cs, gp, s_tab + 2 * (cur << 5), w0, w1, w2, lane, acc, sink);
+  }
+}
+
 template <bool DIFF, bool SPEC, bool VIS>
 // pts: the tile's points already in shared memory (input order), or null to read them from r.
 __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float* s_red, const TilePoints* pts) {
@@ -242,41 +295,10 @@ __device__ void fwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
     }
   }
   float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  const int nsl = r.HWpad >> 5;
-  const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
-  for (int k = 0;; ++k) {
-    const int cur = warp_slot(k, warp, kNW, nsl, ushift);
-    if (cur < 0) break;
-    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
-    if (VIS) {
-      load_vis_words(r, g, valid, cur, w0, w1, w2);
-      if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
-    }
-    const float4* rec = s_tab + 2 * (cur << 5);
-#pragma unroll 1
-    for (int gq = 0; gq < 4; ++gq) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const float4 A = rec[2 * (gq * 8 + j)];
-        if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) continue;
-        const float4 B = rec[2 * (gq * 8 + j) + 1];
-        const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
-        float wd, ws;
-        pair_fwd_weights<DIFF, SPEC>(g, sc, A, B.w, vis, wd, ws);
-        acc[0] = fmaf(B.x, wd, acc[0]);
-        acc[1] = fmaf(B.y, wd, acc[1]);
-        acc[2] = fmaf(B.z, wd, acc[2]);
-        acc[3] = fmaf(B.x, ws, acc[3]);
-        acc[4] = fmaf(B.y, ws, acc[4]);
-        acc[5] = fmaf(B.z, ws, acc[5]);
-      }
-      if (VIS) {
-        w0 >>= 8;
-        w1 >>= 8;
-        w2 >>= 8;
-      }
-    }
-  }
+  if (VIS && warp_single_vertex(g))
+    fwd_tile_slots<DIFF, SPEC, VIS, true>(r, g, valid, sc, s_tab, acc);
+  else
+    fwd_tile_slots<DIFF, SPEC, VIS, false>(r, g, valid, sc, s_tab, acc);
   float* red = s_red + warp * 6 * 32 + lane;
 #pragma unroll
   for (int q = 0; q < 6; ++q) red[q * 32] = acc[q];
@@ -361,57 +383,10 @@ __device__ void bwd_tile(const ReqDesc& r, int tile, const float4* s_tab, float*
   if (SPEC) sc = spec_const(valid ? (pts ? pts->rough[lane] : r.rough[pid]) : 0.f, g);
   const BwdPoint gp{gd0, gd1, gd2, gs0, gs1, gs2};
   BwdAcc acc = {};
-  const int nsl = r.HWpad >> 5;
-  const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
-  const int jsel = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-  for (int k = 0;; ++k) {
-    const int cur = warp_slot(k, warp, kNW, nsl, ushift);
-    if (cur < 0) break;
-    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
-    if (VIS) {
-      load_vis_words(r, g, valid, cur, w0, w1, w2);
-      if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
-    }
-    const float4* rec = s_tab + 2 * (cur << 5);
-#pragma unroll 1
-    for (int gq = 0; gq < 4; ++gq) {
-      float wdj[8], wsj[8];
-      bool live = false;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        wdj[j] = 0.f;
-        wsj[j] = 0.f;
-        const float4 A = rec[2 * (gq * 8 + j)];
-        if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) continue;
-        live = true;
-        const float4 B = rec[2 * (gq * 8 + j) + 1];
-        const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
-        pair_bwd<DIFF, SPEC>(g, sc, gp, A, B, vis, acc, wdj[j], wsj[j]);
-      }
-      if (VIS) {
-        w0 >>= 8;
-        w1 >>= 8;
-        w2 >>= 8;
-      }
-      if (!live) continue;
-      float e[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) e[j] = fmaf(gs0, wsj[j], gd0 * wdj[j]);
-      const float y0 = butterfly8(e, lane);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) e[j] = fmaf(gs1, wsj[j], gd1 * wdj[j]);
-      const float y1 = butterfly8(e, lane);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) e[j] = fmaf(gs2, wsj[j], gd2 * wdj[j]);
-      const float y2 = butterfly8(e, lane);
-      if ((lane & 3) == 0) {
-        const int t = (cur << 5) + gq * 8 + jsel;
-        atomicAdd(r.env_acc + t, (double)y0);
-        atomicAdd(r.env_acc + r.HWpad + t, (double)y1);
-        atomicAdd(r.env_acc + 2 * r.HWpad + t, (double)y2);
-      }
-    }
-  }
+  if (VIS && warp_single_vertex(g))
+    bwd_tile_slots<DIFF, SPEC, VIS, true>(r, g, valid, sc, gp, s_tab, acc);
+  else
+    bwd_tile_slots<DIFF, SPEC, VIS, false>(r, g, valid, sc, gp, s_tab, acc);
   float* red = s_red + warp * NACC * 32 + lane;
   const float* av = &acc.Da0;
 #pragma unroll

@@ -44,8 +44,9 @@ namespace des {
 // Texel table
 // ------------------------------------------------------------------------------------------
 
-// Texel record t: rec[2t] = (l'x, l'y, l'z, d_omega), rec[2t+1] = (L0, L1, L2, d_omega/pi) for
-// t < H*W, zeros for the padding up to a multiple of 32.  `export4` (optional) receives
+// Texel record t: rec[2t] = (l'x, l'y, l'z, d_omega/4), rec[2t+1] = (L0, L1, L2, d_omega/pi) for
+// t < H*W, zeros for the padding up to a multiple of 32.  The 1/4 is the denominator of the GGX
+// term F G D / 4, folded into the table (a power of two: every product it enters is unchanged).  `export4` (optional) receives
 // (x, y, z, d_omega) per texel for des_texel_table.
 __device__ __forceinline__ void table_entry(int t, int H, int W, const float* __restrict__ R,
                                             const float* __restrict__ env, float4* __restrict__ rec,
@@ -61,7 +62,7 @@ __device__ __forceinline__ void table_entry(int t, int H, int W, const float* __
     const float3 l = rotate3(m, texel_direction(iy, ix, W, H));
     const float dw = texel_delta_omega(iy, W, H);
     if (rec != nullptr) {
-      rec[2 * t] = make_float4(l.x, l.y, l.z, dw);
+      rec[2 * t] = make_float4(l.x, l.y, l.z, dw * 0.25f);
       rec[2 * t + 1] = make_float4(env[t], env[HW + t], env[2 * HW + t], dw * kInvPiF);
     }
     if (export4 != nullptr) {
@@ -289,6 +290,42 @@ __global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chu
 // Forward
 // ------------------------------------------------------------------------------------------
 
+// The NW warps of a CTA integrate one tile over their texel slots (mirrored pairs, see warp_slot);
+// a warp's visibility words of its next slot are loaded while it integrates the current one, and a
+// slot whose words are zero for all 32 lanes is skipped.  Tables with more than p.chunk texels are
+// staged chunk by chunk (every warp of the CTA calls this with the same arguments).
+template <bool DIFF, bool SPEC, bool VIS, bool ONEV>
+__device__ __forceinline__ void fwd_tile_sums(const ShadeParams& p, const PointGeom& g, bool valid, const SpecConst& sc,
+                                              float4* s_tab, int nchunks, int warp, int NW, float (&acc)[6]) {
+  const float cs = (g.c0 + g.c1) + g.c2;
+  for (int c = 0; c < nchunks; ++c) {
+    const int cbase = c * p.chunk;
+    const int clen = min(p.chunk, p.HWpad - cbase);
+    if (nchunks > 1) {
+      __syncthreads();
+      stage_table(s_tab, p.table, cbase, clen);
+      __syncthreads();
+    }
+    const int nsl = clen >> 5;
+    const int ushift = ((nsl + 1) >> 1) >= NW ? 1 : 0;
+    const int gslot0 = cbase >> 5;
+    uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
+    int sl = warp_slot(0, warp, NW, nsl, ushift);
+    if (VIS && sl >= 0) load_vis_words<ONEV>(p, g, valid, gslot0 + sl, n0, n1, n2);
+    for (int k = 1; sl >= 0; ++k) {
+      const int cur = sl;
+      sl = warp_slot(k, warp, NW, nsl, ushift);
+      const uint32_t w0 = n0, w1 = n1, w2 = n2;
+      if (VIS) {
+        if (sl >= 0) load_vis_words<ONEV>(p, g, valid, gslot0 + sl, n0, n1, n2);
+        // skip a 32-point x 32-texel tile that is fully occluded for every lane
+        if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
+      }
+      fwd_slot<DIFF, SPEC, VIS, ONEV>(g, sc, cs, s_tab + 2 * (cur << 5), w0, w1, w2, acc);
+    }
+  }
+}
+
 template <bool DIFF, bool SPEC, bool VIS>
 __global__ void __maxnreg__(64) des_fwd_kernel(const ShadeParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -318,83 +355,32 @@ __global__ void __maxnreg__(64) des_fwd_kernel(const ShadeParams p) {
     SpecConst sc;
     if (SPEC) sc = spec_const(valid ? p.rough[pid] : 0.f, g);
 
-    float D0 = 0.f, D1 = 0.f, D2 = 0.f;  // sum L * diffuse weight  (white diffuse shading)
-    float S0 = 0.f, S1 = 0.f, S2 = 0.f;  // sum L * specular weight
-
-    for (int c = 0; c < nchunks; ++c) {
-      const int cbase = c * p.chunk;
-      const int clen = min(p.chunk, p.HWpad - cbase);
-      if (nchunks > 1) {
-        __syncthreads();
-        stage_table(s_tab, p.table, cbase, clen);
-        __syncthreads();
-      }
-      const int nsl = clen >> 5;
-      const int ushift = ((nsl + 1) >> 1) >= NW ? 1 : 0;
-      const int gslot0 = cbase >> 5;
-      uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
-      int sl = warp_slot(0, warp, NW, nsl, ushift);
-      if (VIS && sl >= 0) load_vis_words(p, g, valid, gslot0 + sl, n0, n1, n2);
-      for (int k = 1; sl >= 0; ++k) {
-        const int cur = sl;
-        sl = warp_slot(k, warp, NW, nsl, ushift);
-        uint32_t w0 = n0, w1 = n1, w2 = n2;
-        if (VIS) {
-          if (sl >= 0) load_vis_words(p, g, valid, gslot0 + sl, n0, n1, n2);
-          // skip a 32-point x 32-texel tile that is fully occluded for every lane
-          if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
-        }
-        const float4* rec = s_tab + 2 * (cur << 5);
-#pragma unroll 1
-        for (int gq = 0; gq < 4; ++gq) {
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const float4 A = rec[2 * (gq * 8 + j)];
-            // texel below the horizon of all 32 points: it adds nothing to any of them
-            if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) continue;
-            const float4 B = rec[2 * (gq * 8 + j) + 1];
-            const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
-            float wd, ws;
-            pair_fwd_weights<DIFF, SPEC>(g, sc, A, B.w, vis, wd, ws);
-            if (DIFF) {
-              D0 = fmaf(B.x, wd, D0);
-              D1 = fmaf(B.y, wd, D1);
-              D2 = fmaf(B.z, wd, D2);
-            }
-            if (SPEC) {
-              S0 = fmaf(B.x, ws, S0);
-              S1 = fmaf(B.y, ws, S1);
-              S2 = fmaf(B.z, ws, S2);
-            }
-          }
-          if (VIS) {
-            w0 >>= 8;
-            w1 >>= 8;
-            w2 >>= 8;
-          }
-        }
-      }
-    }
+    // acc[0..2] = sum L * diffuse weight (white diffuse shading), acc[3..5] = sum L * specular weight
+    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (VIS && warp_single_vertex(g))
+      fwd_tile_sums<DIFF, SPEC, VIS, true>(p, g, valid, sc, s_tab, nchunks, warp, NW, acc);
+    else
+      fwd_tile_sums<DIFF, SPEC, VIS, false>(p, g, valid, sc, s_tab, nchunks, warp, NW, acc);
 
     // combine the NW texel ranges in warp order
     float* red = s_red + warp * 6 * 32 + lane;
-    red[0] = D0; red[32] = D1; red[64] = D2;
-    red[96] = S0; red[128] = S1; red[160] = S2;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) red[q * 32] = acc[q];
     __syncthreads();
     if (warp == 0 && valid) {
-      float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       for (int w = 0; w < NW; ++w) {
         const float* r = s_red + w * 6 * 32 + lane;
 #pragma unroll
-        for (int q = 0; q < 6; ++q) acc[q] += r[q * 32];
+        for (int q = 0; q < 6; ++q) sum[q] += r[q * 32];
       }
 #pragma unroll
       for (int ch = 0; ch < 3; ++ch) {
         float out = 0.f;
-        if (DIFF) out = p.albedo[3 * pid + ch] * acc[ch];
-        if (SPEC) out = fmaf(p.spec[3 * pid + ch], acc[3 + ch], out);
+        if (DIFF) out = p.albedo[3 * pid + ch] * sum[ch];
+        if (SPEC) out = fmaf(p.spec[3 * pid + ch], sum[3 + ch], out);
         p.shading[3 * pid + ch] = out;
-        if (p.white != nullptr) p.white[3 * pid + ch] = acc[ch];
+        if (p.white != nullptr) p.white[3 * pid + ch] = sum[ch];
       }
     }
     __syncthreads();
@@ -406,6 +392,53 @@ __global__ void __maxnreg__(64) des_fwd_kernel(const ShadeParams p) {
 // ------------------------------------------------------------------------------------------
 // Backward (point gradients + env-map gradient in one pass)
 // ------------------------------------------------------------------------------------------
+
+// As fwd_tile_sums, for the adjoint: the point's sums go to acc, the env-map gradient of each
+// 8-texel group (summed over the 32 lanes) to the CTA's FP64 accumulator env_acc (row stride env_ld;
+// indexed by the texel within the staged chunk when the accumulator is in shared memory, by the
+// texel of the whole map otherwise).
+template <bool DIFF, bool SPEC, bool VIS, bool ONEV>
+__device__ __forceinline__ void bwd_tile_sums(const ShadeParams& p, const PointGeom& g, bool valid, const SpecConst& sc,
+                                              const BwdPoint& gp, float4* s_tab, double* env_acc, int env_ld,
+                                              int nchunks, int warp, int NW, int lane, BwdAcc& acc) {
+  const float cs = (g.c0 + g.c1) + g.c2;
+  const int jsel = butterfly_texel(lane);
+  for (int c = 0; c < nchunks; ++c) {
+    const int cbase = c * p.chunk;
+    const int clen = min(p.chunk, p.HWpad - cbase);
+    if (nchunks > 1) {
+      __syncthreads();
+      stage_table(s_tab, p.table, cbase, clen);
+      __syncthreads();
+    }
+    const int nsl = clen >> 5;
+    const int ushift = ((nsl + 1) >> 1) >= NW ? 1 : 0;
+    const int gslot0 = cbase >> 5;
+    const int ebase = p.env_in_smem ? 0 : cbase;
+    uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
+    int sl = warp_slot(0, warp, NW, nsl, ushift);
+    if (VIS && sl >= 0) load_vis_words<ONEV>(p, g, valid, gslot0 + sl, n0, n1, n2);
+    for (int k = 1; sl >= 0; ++k) {
+      const int cur = sl;
+      sl = warp_slot(k, warp, NW, nsl, ushift);
+      const uint32_t w0 = n0, w1 = n1, w2 = n2;
+      if (VIS) {
+        if (sl >= 0) load_vis_words<ONEV>(p, g, valid, gslot0 + sl, n0, n1, n2);
+        if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
+      }
+      double* const eslot = env_acc + ebase + (cur << 5) + jsel;
+      auto sink = [&](int gq, float y0, float y1, float y2) {
+        if ((lane & 3) == 0) {
+          double* a = eslot + gq * 8;
+          a[0] += (double)y0;
+          a[env_ld] += (double)y1;
+          a[2 * env_ld] += (double)y2;
+        }
+      };
+      bwd_slot<DIFF, SPEC, VIS, ONEV>(g, sc, cs, gp, s_tab + 2 * (cur << 5), w0, w1, w2, lane, acc, sink);
+    }
+  }
+}
 
 template <bool DIFF, bool SPEC, bool VIS>
 __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadeParams p) {
@@ -464,75 +497,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
 
     BwdAcc acc = {};
     const BwdPoint gp{gd0, gd1, gd2, gs0, gs1, gs2};
-
-    for (int c = 0; c < nchunks; ++c) {
-      const int cbase = c * p.chunk;
-      const int clen = min(p.chunk, p.HWpad - cbase);
-      if (nchunks > 1) {
-        __syncthreads();
-        stage_table(s_tab, p.table, cbase, clen);
-        __syncthreads();
-      }
-      const int nsl = clen >> 5;
-      const int ushift = ((nsl + 1) >> 1) >= NW ? 1 : 0;
-      const int gslot0 = cbase >> 5;
-      const int ebase = p.env_in_smem ? 0 : cbase;
-      uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
-      int sl = warp_slot(0, warp, NW, nsl, ushift);
-      if (VIS && sl >= 0) load_vis_words(p, g, valid, gslot0 + sl, n0, n1, n2);
-      for (int k = 1; sl >= 0; ++k) {
-        const int cur = sl;
-        sl = warp_slot(k, warp, NW, nsl, ushift);
-        uint32_t w0 = n0, w1 = n1, w2 = n2;
-        if (VIS) {
-          if (sl >= 0) load_vis_words(p, g, valid, gslot0 + sl, n0, n1, n2);
-          if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
-        }
-        const float4* rec = s_tab + 2 * (cur << 5);
-#pragma unroll 1
-        for (int gq = 0; gq < 4; ++gq) {
-          float wdj[8], wsj[8];
-          bool live = false;  // warp-uniform: some texel of the group is above some lane's horizon
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            wdj[j] = 0.f;
-            wsj[j] = 0.f;
-            const float4 A = rec[2 * (gq * 8 + j)];
-            // texel below the horizon of all 32 points: no contribution to any output
-            if (!__any_sync(0xffffffffu, dot3(g.nx, g.ny, g.nz, A.x, A.y, A.z) > 0.f)) continue;
-            live = true;
-            const float4 B = rec[2 * (gq * 8 + j) + 1];
-            const float vis = VIS ? vis_weight(w0, w1, w2, 1u << j, g.c0, g.c1, g.c2) : 1.f;
-            pair_bwd<DIFF, SPEC>(g, sc, gp, A, B, vis, acc, wdj[j], wsj[j]);
-          }
-          if (VIS) {
-            w0 >>= 8;
-            w1 >>= 8;
-            w2 >>= 8;
-          }
-          if (!live) continue;
-          // env-map gradient of these 8 texels: per lane e = gd * wd + gs * ws, summed over lanes
-          const int t0 = ebase + (cur << 5) + gq * 8;
-          const int jsel = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-          float e[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) e[j] = fmaf(gs0, wsj[j], gd0 * wdj[j]);
-          const float y0 = butterfly8(e, lane);
-#pragma unroll
-          for (int j = 0; j < 8; ++j) e[j] = fmaf(gs1, wsj[j], gd1 * wdj[j]);
-          const float y1 = butterfly8(e, lane);
-#pragma unroll
-          for (int j = 0; j < 8; ++j) e[j] = fmaf(gs2, wsj[j], gd2 * wdj[j]);
-          const float y2 = butterfly8(e, lane);
-          if ((lane & 3) == 0) {
-            double* acc = env_acc + t0 + jsel;
-            acc[0] += (double)y0;
-            acc[env_ld] += (double)y1;
-            acc[2 * env_ld] += (double)y2;
-          }
-        }
-      }
-    }
+    if (VIS && warp_single_vertex(g))
+      bwd_tile_sums<DIFF, SPEC, VIS, true>(p, g, valid, sc, gp, s_tab, env_acc, env_ld, nchunks, warp, NW, lane, acc);
+    else
+      bwd_tile_sums<DIFF, SPEC, VIS, false>(p, g, valid, sc, gp, s_tab, env_acc, env_ld, nchunks, warp, NW, lane, acc);
 
     // combine the NW texel ranges in warp order, then finish the per-point chain rule
     float* red = s_red + warp * NACC * 32 + lane;
@@ -756,6 +724,11 @@ std::atomic<cudaEvent_t> g_timing_stop{nullptr};
 void set_timing_events(cudaEvent_t start, cudaEvent_t stop) {
   g_timing_start.store(start);
   g_timing_stop.store(stop);
+}
+
+void timing_events(cudaEvent_t& start, cudaEvent_t& stop) {
+  start = g_timing_start.load();
+  stop = g_timing_stop.load();
 }
 
 namespace {

@@ -300,8 +300,9 @@ int des_blur_envmap_forward(int32_t H, int32_t W, int32_t C, int32_t tar_H, int3
 int des_texel_table(int32_t H, int32_t W, const float* light2obj_rotmat, float* table_out, des_stream_t stream);
 
 /* Instrumentation.  While both events are set (non-NULL cudaEvent_t handles), every shading call
- * records `start_event` on its stream immediately before its main kernel (the forward sum or the
- * fused adjoint) and `stop_event` immediately after it, so the caller can time that kernel alone.
+ * records `start_event` on its stream immediately before its main kernel (the forward sum, the
+ * fused adjoint, or the first tensor-core pass of des_relight_multienv) and `stop_event`
+ * immediately after it, so the caller can time that kernel alone.
  * Process-wide; pass NULL, NULL to turn it off. */
 int des_set_timing_events(void* start_event, void* stop_event);
 
