@@ -15,7 +15,11 @@ the reported time is the max over ranks.
 
 At N = 1 the line also carries a serving leg ("serving"): 2000 requests (Poisson 5k/s, 1k-500k
 points, 16x32 or 32x64 env, visibility on/off, 30% with gradients) through the continuous-batching
-server against the same arrivals served one at a time by the plain operators (--no-serve skips it).
+server against the same arrivals served one at a time by the plain operators (--no-serve skips it);
+a relight leg ("relight"): 262,144 points x 64 env maps x 16x32 on the tensor cores against 64
+plain FP32 passes (--no-relight skips it); and the same fwd+bwd step with the visibility of each
+point interpolated over a random triangle ("mesh_layout") -- the headline workload gives every
+point its own visibility row (barycentrics (1, 0, 0)), as a per-point visibility mask does.
 
 ``--impl reference`` times the CPU restatement of the reference's sum (the reference has no
 CPU path of its own) on the host cores, on a bounded sample of the same workload.
@@ -55,6 +59,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-relight", action="store_true", help="skip the K-env-map relight leg")
     return ap.parse_args()
 
 
@@ -227,6 +232,119 @@ def run_reference_arm(args):
 # ------------------------------------------------------------------------------------------------
 # GPU arm
 # ------------------------------------------------------------------------------------------------
+
+def bf16_peak():
+    """Dense bf16 tensor peak (TFLOP/s) for a kernel timed alone: the burst figure of
+    MEASURED_PEAKS.json, else this pool's earlier measurement."""
+    peaks = measured_peaks()
+    for k in ("bf16_tflops", "bf16_tflops_burst"):
+        if k in peaks:
+            return float(peaks[k]), f"{k} of MEASURED_PEAKS.json (measured)"
+    return 1590.0, "fallback 1.59 PFLOP/s (earlier measurement on this pool; MEASURED_PEAKS.json absent)"
+
+
+def relight_leg(des, wl, dev, flush, peak_tinst, steps=10, warmup=3):
+    """K-env-map relighting (262,144 points x 64 maps x 16x32, 512-bit visibility) on tcgen05:
+    the whole op (table, ordering, radiance tiles, tensor-core pass) and its tensor-core kernel alone,
+    timed with CUDA events with the L2 flushed between passes; against 64 plain FP32 forward passes."""
+    c = wl.CONFIGS["multienv-262k"]
+    inp = wl.make_inputs(c["P"], c["H"], c["W"], c["seed"], sigma=c["sigma"], rough=c["rough"], vis_p=c["vis_p"],
+                         env_count=c["K"])
+    d = inp.to(dev)
+    P, H, W, K = c["P"], c["H"], c["W"], c["K"]
+    HW = H * W
+    vis = (d.face_vertex_list, d.nearest_triangle_id, d.barycentric_coord, d.visibility)
+    base = (d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness)
+
+    def fused():
+        return des.relight_multienv(*base, d.envmap, d.light2obj_rotmat, *vis, True, True)
+
+    def plain():
+        return torch.stack([des.bruteforce_specularvisibility_shader_forward2(
+            *base, d.envmap[k], d.light2obj_rotmat, *vis, True)[0] for k in range(K)], dim=1)
+
+    for _ in range(warmup):
+        fused()
+    torch.cuda.synchronize()
+    op_ms, kern_ms = [], []
+    for i in range(steps):
+        flush.fill_(float(i))
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        for x in e[2:]:
+            x.record()  # torch creates events lazily
+        des.set_timing_events(e[2].cuda_event, e[3].cuda_event)
+        e[0].record()
+        out = fused()
+        e[1].record()
+        des.set_timing_events(0, 0)
+        torch.cuda.synchronize()
+        op_ms.append(e[0].elapsed_time(e[1]))
+        kern_ms.append(e[2].elapsed_time(e[3]))
+    ref = plain()
+    torch.cuda.synchronize()
+    p_ms = []
+    for i in range(3):
+        flush.fill_(float(i))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        plain()
+        b.record()
+        torch.cuda.synchronize()
+        p_ms.append(a.elapsed_time(b))
+    scale = float(ref.abs().max())
+    err = float(((out - ref).abs() / (ref.abs() + 1e-3 * scale)).max())
+    op, kern, pl = float(np.median(op_ms)), float(np.median(kern_ms)), float(np.median(p_ms))
+    build_tinst = P * HW * INSTR_FWD_VIS / (kern * 1e-3) / 1e12
+    flops_alg = 2.0 * P * HW * 3 * K  # one [P x HW] x [HW x 3K] product per pass
+    flops_exec = 3 * flops_alg        # BF16 hi*hi + lo*hi + hi*lo
+    peak_tc, peak_src = bf16_peak()
+    return {
+        "workload": f"multienv-262k: {P} points x {K} env maps x {H}x{W}, 512-bit visibility, BF16 hi/lo on tcgen05",
+        "ms_per_pass": op, "kernel_ms": kern, "value": P * HW * K / (op * 1e-3), "unit": "point*texel*map/s",
+        "weight_build": {"bound": "fp32", "work": f"{INSTR_FWD_VIS} FP32-pipe instr per point*texel pair",
+                         "achieved": build_tinst, "peak": peak_tinst, "unit": "T FP32-pipe instr/s",
+                         "frac": build_tinst / peak_tinst},
+        "tensor": {"achieved": flops_exec / (kern * 1e-3) / 1e12, "algorithmic": flops_alg / (kern * 1e-3) / 1e12,
+                   "peak": peak_tc, "unit": "TFLOP/s", "frac": flops_exec / (kern * 1e-3) / 1e12 / peak_tc,
+                   "peak_source": peak_src},
+        "max_rel_err_vs_plain_fp32": err,
+        "error_note": "per element |d| / (|plain| + 1e-3 max|plain|) against 64 plain FP32 forward passes; the FP64 "
+                      "oracle comparison is tests/test_gpu_relight.py",
+        "plain_64x_ms": pl, "speedup_vs_plain": pl / op,
+        "l2": "256 MiB buffer rewritten between timed passes (outside the timed events)",
+    }
+
+
+def mesh_layout_step(des, wl, dev, flush, steps=10, warmup=3):
+    """The same fwd+bwd step with visibility interpolated over random triangles (three vertex words
+    per point and texel) instead of one visibility row per point."""
+    c = wl.CONFIGS[CONFIG_NAME]
+    d = wl.make_inputs(c["P"], c["H"], c["W"], c["seed"], sigma=c["sigma"], rough=c["rough"], vis_p=c["vis_p"],
+                       vis_layout="mesh").to(dev)
+    vis = (d.face_vertex_list, d.nearest_triangle_id, d.barycentric_coord, d.visibility)
+
+    def step():
+        torch.autograd.graph.increment_version(d.normal)
+        des.bruteforce_specularvisibility_shader_forward2(d.normal, d.view_dir, d.albedo, d.specular_albedo,
+                                                          d.roughness, d.envmap, d.light2obj_rotmat, *vis, True)
+        des.bruteforce_specularvisibility_shader_backward2(d.grad_shading, d.grad_diffuse_shading, d.normal,
+                                                           d.view_dir, d.albedo, d.specular_albedo, d.roughness,
+                                                           d.envmap, d.light2obj_rotmat, *vis, True)
+
+    for _ in range(warmup):
+        step()
+    ms = []
+    for i in range(steps):
+        flush.fill_(float(i))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        step()
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    m = float(np.mean(ms))
+    return {"ms_per_step": m, "value": c["P"] * c["H"] * c["W"] / (m * 1e-3), "unit": UNIT,
+            "layout": "random triangles over P/2 vertices, Dirichlet barycentrics (three words per point and slot)"}
 
 def main():
     args = parse()
@@ -480,6 +598,12 @@ def main():
                     "work": f"{INSTR_FWD_VIS} instr/pair"},
     }
 
+    relight = mesh = None
+    if rank == 0 and world == 1:
+        mesh = mesh_layout_step(des, wl, dev, flush)
+        if not args.no_relight:
+            relight = relight_leg(des, wl, dev, flush, peak_tinst)
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         # served p50/p99 against serial plain launches on one arrival schedule (2000 requests, Poisson 5k/s)
@@ -503,6 +627,8 @@ def main():
             "e2e": e2e,
             "clocks": clocks,
             "serving": serving,
+            "relight": relight,
+            "mesh_layout": mesh,
             "fwd_ms": float(np.mean(fwd_ms)), "bwd_ms": float(np.mean(bwd_ms)),
         }
         print(json.dumps(line))

@@ -210,7 +210,37 @@ def test_against_reference_live(des, reference_ext, name, op, layout):
     ref = run_op(reference_ext, op, d)
     table = des.texel_table(c["H"], c["W"], d.light2obj_rotmat).cpu().numpy()
     exact = oracle_outputs(op, inp, True, True, table)
+    _record_parity(name, got, ref, exact)
     check_against_reference(got, ref, exact, name)
+
+
+def _raw_stats(a, b):
+    """(max|a - b| / max|b|, max over elements of |a - b| / |b|) with no allowance and no floor
+    (elements where both are exactly zero count as equal)."""
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    d = np.abs(a - b)
+    scale = np.abs(b).max()
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rel = np.where(d == 0, 0.0, d / np.abs(b))
+    return float(d.max() / scale) if scale > 0 else float(d.max()), float(rel.max())
+
+
+def _record_parity(name, got, ref, exact):
+    """The literal comparison against the reference (no allowance) per output, beside the same
+    statistics of the reference and of this build against the FP64 oracle.  Printed, and appended
+    as JSON to $DES_PERF_OUT when set."""
+    import json
+    rows = {}
+    for k in ref:
+        t_or, e_or = _raw_stats(got[k], ref[k])
+        t_rx, e_rx = _raw_stats(ref[k], exact[k])
+        t_ox, e_ox = _raw_stats(got[k], exact[k])
+        rows[k] = {"ours_vs_ref": [t_or, e_or], "ref_vs_fp64": [t_rx, e_rx], "ours_vs_fp64": [t_ox, e_ox]}
+    line = {"parity_case": name, "stats": "[max|d|/max|ref|, max elementwise |d|/|ref|]", "outputs": rows}
+    print(json.dumps(line))
+    if os.environ.get("DES_PERF_OUT"):
+        with open(os.environ["DES_PERF_OUT"], "a") as f:
+            f.write(json.dumps(line) + "\n")
 
 
 @pytest.mark.parametrize("op,ed,es,layout", [
