@@ -288,7 +288,7 @@ __device__ __forceinline__ bool build_tile(const Params& p, const float4* s_tab,
 // ---- main kernel ---------------------------------------------------------------------------
 
 template <bool DIFF, bool SPEC, bool VIS>
-__global__ void __maxnreg__(88) relight_kernel(const Params p) {
+__global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int HWpad = p.pt.HWpad;
   const Smem L = smem_layout(HWpad, p.kpad);
@@ -453,8 +453,8 @@ __global__ void __maxnreg__(88) relight_kernel(const Params p) {
     // ------------------------------------------------------------------ radiance bulk copies
     if (lane == 0) {
       uint32_t q = 0;
-      uint32_t last_use[2] = {0u, 0u};
-      bool issued[2] = {false, false};
+      // copies issued so far into buffer 0 and buffer 1 (the last one into buffer b used phase n_b - 1)
+      uint32_t n_b0 = 0u, n_b1 = 0u;
       for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
         bool ok = true;
         for (int st = 0; st < p.nst; ++st, ++q) {
@@ -465,16 +465,17 @@ __global__ void __maxnreg__(88) relight_kernel(const Params p) {
           }
           mbar_arrive_expect_tx(&full_b[b], b_stage);
           bulk_g2s(b_base + b * b_stage, p.bprep + (size_t)st * b_stage, b_stage, &full_b[b]);
-          issued[b] = true;
-          last_use[b] = u;
+          if (b == 0u) ++n_b0;
+          else ++n_b1;
         }
         if (!ok) break;
       }
       // never leave a bulk copy in flight: wait (bounded) for the last one into each buffer
       for (int b = 0; b < 2; ++b) {
-        if (!issued[b]) continue;
+        const uint32_t n_issued = b == 0 ? n_b0 : n_b1;
+        if (n_issued == 0u) continue;
         const long long t0 = global_ns();
-        while (!mbar_try_wait(&full_b[b], last_use[b] & 1u)) {
+        while (!mbar_try_wait(&full_b[b], (n_issued - 1u) & 1u)) {
           if (global_ns() - t0 > kWaitNs) {
             atomicOr(err, kErrTimeout);
             break;
