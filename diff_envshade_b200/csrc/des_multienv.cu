@@ -1,30 +1,34 @@
 // Multi-env-map relighting on the 5th-generation tensor cores (tcgen05, sm_100a).
 //
-// out[p, k, c] = sum_t A_c[p, t] * L_k[c, t],   A_c = albedo_c * w_d + specular_c * w_s,
+// out[p, k, c] = albedo_c[p] sum_t w_d[p, t] L_k[c, t] + specular_c[p] sum_t w_s[p, t] L_k[c, t],
 // where w_d = vis * max(n.l, 0) * dw / pi and w_s = vis * dw * F G D / 4 are the per-(point, texel)
 // weights of the reference's forward sum (bruteforce_shader.cu:2171-2236).  For one env map this is
-// the shading output of bruteforce_specularvisibility_shader_forward2; for K env maps it is, per
-// colour channel, a [points x texels] x [texels x K] product, which runs on the tensor cores.
+// the shading output of bruteforce_specularvisibility_shader_forward2; for K env maps the two sums
+// are [points x texels] x [texels x 3K] products (the weights do not depend on the colour channel,
+// so one weight matrix per term serves all three channels), which run on the tensor cores; the
+// albedos are applied per point when the accumulators are read out.
 //
 // Precision: the weights are computed in FP32 and split into BF16 hi + lo parts, the radiance too;
 // each tile accumulates hi*hi + lo*hi + hi*lo in FP32 (error ~2^-16 relative).  DES_RELIGHT_BF16
 // keeps only hi*hi (plain BF16 inputs, error ~2^-8 relative per term).
 //
 // Kernel structure (one persistent CTA per SM, 22 warps):
-//   warps 0-15  builders: per 32-texel stage, 128 points x 32 texels of A_c (3 channels, hi and lo)
-//               written to shared memory in the UMMA K-major no-swizzle canonical layout
-//               (8-row x 16-byte core matrices, 128 B each); four threads per point row, one
-//               8-texel chunk each (sixteen warps hide the latency of the weight build better
-//               than eight: the build, not the MMA, bounds the kernel);
-//   warp 16     allocates 512 TMEM columns; lane 0 issues tcgen05.mma (M=128, N=Kpad, K=16) and
-//               tcgen05.commit to the stage-empty / accumulator-full mbarriers;
-//   warps 17-20 epilogue: tcgen05.ld of the finished tile (32 TMEM lanes per warp) -> global;
-//   warp 21     lane 0 streams the prepared BF16 radiance tile of each stage with cp.async.bulk
+//   warps 0-15  builders: per 32-texel stage, the weights of 128 points x 32 texels (W_d and W_s,
+//               hi and lo) written to shared memory in the UMMA K-major no-swizzle canonical layout
+//               (8-row x 16-byte core matrices, 128 B each); four threads per point row, one 8-texel
+//               chunk each;
+//   warp 16     allocates 512 TMEM columns; lane 0 issues tcgen05.mma (M=128, N=3K padded, K=16)
+//               and tcgen05.commit to the stage-empty / accumulator-full mbarriers;
+//   warps 17-20 epilogue: tcgen05.ld of the finished tile (32 TMEM lanes per warp), albedos applied,
+//               -> global;
+//   warp 21     lane 0 streams the prepared BF16 radiance tiles of each stage with cp.async.bulk
 //               (a plain bulk copy from this GPU's memory; no multicast).
-// Two shared-memory stages and two TMEM accumulator buffers (2 x 3 x Kpad columns) let the weight
-// build, the MMAs and the epilogue overlap.  Every mbarrier wait is bounded (2 s of %globaltimer):
-// on timeout the CTA sets the workspace error word, stops issuing work, waits (bounded) for its
-// own bulk copies and MMAs in flight, frees its TMEM and returns.
+// A ring of three shared-memory stages (two for the largest maps) lets each builder warp run up to
+// two stages ahead of the slowest one -- their per-stage work differs with the horizon skip -- while
+// the MMAs of earlier stages run; two TMEM accumulator sets overlap a tile's epilogue with the next
+// tile's MMAs when their columns fit.  Every mbarrier wait is bounded (2 s of %globaltimer): on
+// timeout the CTA sets the workspace error word, stops issuing work, waits (bounded) for its own
+// bulk copies and MMAs in flight, frees its TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -42,7 +46,7 @@ namespace relight {
 
 constexpr int kTileM = 128;                  // points per tile (UMMA M)
 constexpr int kStageT = 32;                  // texels per stage (one visibility slot)
-constexpr int kNStage = 2;                   // shared-memory ring depth
+constexpr int kMaxStages = 3;                // shared-memory ring depth (3 when it fits, else 2)
 constexpr int kEnvBlock = 64;                // env maps per pass
 constexpr int kBuilderThreads = 512;         // warps 0-15
 constexpr int kCtrlWarp = 16;
@@ -56,10 +60,14 @@ constexpr unsigned kErrTimeout = 2u;
 
 struct Params {
   ShadeParams pt;         // point inputs, texel table, control words
-  const uint8_t* bprep;   // [nst][3][2][kpad x 32] BF16 radiance tiles (canonical layout)
+  const uint8_t* bprep;   // [nst][hl][ncols x 32] BF16 radiance tiles (canonical layout), row = c * kpad + k
   float* out;             // [P][ldo]; this pass writes columns 3*kbase .. 3*(kbase + kblock) - 1
   int64_t ldo;
   int kbase, kblock, kpad, nst, ntiles;
+  int ncols;              // 3 * kpad: the MMA's N (colour channel major, env map minor)
+  int nmat;               // weight matrices per stage: Lambert and/or GGX (1 or 2)
+  int nstage;             // ring depth (2 or 3)
+  int nacc;               // TMEM accumulator sets (2 when 2 * nmat * ncols columns fit, else 1)
   bool split, vec_store;
 };
 
@@ -69,18 +77,21 @@ struct Smem {  // byte offsets into dynamic shared memory
 
 __host__ __device__ inline uint32_t align_to(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
-__host__ __device__ inline Smem smem_layout(int HWpad, int kpad) {
+// Bytes of one stage of radiance tiles: hi and lo, ncols x 32 texels of BF16.
+__host__ __device__ inline uint32_t bprep_stage_bytes(int kpad) { return 2u * 3u * (uint32_t)kpad * kStageT * 2u; }
+// Bytes of one stage of weight tiles: nmat matrices, hi and lo.
+__host__ __device__ inline uint32_t a_stage_bytes(int nmat) { return (uint32_t)nmat * 2u * kATile; }
+
+__host__ __device__ inline Smem smem_layout(int HWpad, int kpad, int nmat, int nstage) {
   Smem s;
   s.tab = 0;
   s.a = align_to((uint32_t)HWpad * 32, 1024);
-  s.b = s.a + kNStage * 3 * 2 * kATile;
-  s.bar = align_to(s.b + kNStage * 3 * 2 * (uint32_t)kpad * kStageT * 2, 64);
+  s.b = s.a + (uint32_t)nstage * a_stage_bytes(nmat);
+  s.bar = align_to(s.b + (uint32_t)nstage * bprep_stage_bytes(kpad), 64);
   s.misc = s.bar + 16 * 8;
   s.total = s.misc + 64;
   return s;
 }
-
-__host__ __device__ inline uint32_t bprep_stage_bytes(int kpad) { return 3u * 2u * (uint32_t)kpad * kStageT * 2u; }
 
 // ---- PTX helpers --------------------------------------------------------------------------
 
@@ -173,6 +184,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -197,46 +216,50 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_
 
 // ---- radiance preparation ------------------------------------------------------------------
 
-// bprep[st][c][hl][canon(k, j)] = hi/lo BF16 of L[kbase + k][c][st*32 + j] (zero outside the map / block).
+// bprep[st][hl][canon(c * kpad + k, j)] = hi/lo BF16 of L[kbase + k][c][st*32 + j] (zero outside the map
+// and the block): per stage one [3 kpad x 32] B operand, rows ordered by colour channel, then env map.
 __global__ void prep_kernel(const float* __restrict__ env, int HW, int nst, int kbase, int kblock, int kpad,
                             uint8_t* __restrict__ bprep) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // over nst * 3 * kpad * 32
-  const int total = nst * 3 * kpad * kStageT;
+  const int ncols = 3 * kpad;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // over nst * ncols * 32
+  const int total = nst * ncols * kStageT;
   if (idx >= total) return;
   const int j = idx % kStageT;
-  const int k = (idx / kStageT) % kpad;
-  const int c = (idx / (kStageT * kpad)) % 3;
-  const int st = idx / (kStageT * kpad * 3);
+  const int row = (idx / kStageT) % ncols;
+  const int st = idx / (kStageT * ncols);
+  const int c = row / kpad, k = row - c * kpad;
   const int t = st * kStageT + j;
   float L = 0.f;
   if (k < kblock && t < HW) L = env[((size_t)(kbase + k) * 3 + c) * HW + t];
   const __nv_bfloat16 hi = __float2bfloat16_rn(L);
   const __nv_bfloat16 lo = __float2bfloat16_rn(L - __bfloat162float(hi));
-  const size_t tile = (size_t)kpad * kStageT * 2;
-  uint8_t* base = bprep + (size_t)st * bprep_stage_bytes(kpad) + (size_t)c * 2 * tile;
-  *reinterpret_cast<__nv_bfloat16*>(base + canon_off(k, j)) = hi;
-  *reinterpret_cast<__nv_bfloat16*>(base + tile + canon_off(k, j)) = lo;
+  uint8_t* base = bprep + (size_t)st * bprep_stage_bytes(kpad);
+  *reinterpret_cast<__nv_bfloat16*>(base + canon_off(row, j)) = hi;
+  *reinterpret_cast<__nv_bfloat16*>(base + (size_t)ncols * kStageT * 2 + canon_off(row, j)) = lo;
 }
 
 // ---- weight builders -----------------------------------------------------------------------
 
 // One builder thread's share of one tile: for every 32-texel stage, the 8-texel chunk `quarter` of
-// point row `row` -- A_c = albedo_c wd + specular_c ws for c = 0..2, as BF16 hi and lo parts -- into
-// the stage's shared-memory A tiles (K-major canonical layout).  Texels are taken in pairs: a pair
-// below the horizon of the warp's 32 (ordered) points gets zero weights after one vote, otherwise
-// both are evaluated side by side.  The visibility words of the next stage are loaded while this one
-// is built.  q counts the stages this thread has filled (ring position).  Returns false when the CTA
-// gave up waiting (the whole warp leaves together).
+// point row `row` of the weight matrices -- W_d = the Lambert weight wd and W_s = the GGX weight ws
+// (whichever of the two terms is on), as BF16 hi and lo parts -- into the stage's shared-memory A
+// tiles (K-major canonical layout).  The albedos are applied per point in the epilogue, so one pair
+// of matrices serves all three colour channels.  Texels are taken in pairs: a pair below the horizon
+// of the warp's 32 (ordered) points gets zero weights after one vote, otherwise both are evaluated
+// side by side.  The visibility words of the next stage are loaded while this one is built.  q counts
+// the stages this thread has filled (ring position).  Returns false when the CTA gave up waiting (the
+// whole warp leaves together).
 template <bool DIFF, bool SPEC, bool VIS, bool ONEV>
 __device__ __forceinline__ bool build_tile(const Params& p, const float4* s_tab, const PointGeom& g, bool valid,
-                                           const SpecConst& sc, const float (&alb)[3], const float (&spc)[3], int row,
-                                           int quarter, uint32_t& q, uint32_t a_base, uint64_t* full_a,
-                                           uint64_t* empty, volatile int* s_abort, unsigned* err) {
+                                           const SpecConst& sc, int row, int quarter, uint32_t& q, uint32_t a_base,
+                                           uint64_t* full_a, uint64_t* empty, volatile int* s_abort, unsigned* err) {
+  constexpr int NMAT = (DIFF ? 1 : 0) + (SPEC ? 1 : 0);
   const float cs = (g.c0 + g.c1) + g.c2;
+  const uint32_t nstage = (uint32_t)p.nstage;
   uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
   if (VIS) load_vis_words<ONEV>(p.pt, g, valid, 0, n0, n1, n2);
   for (int st = 0; st < p.nst; ++st, ++q) {
-    const uint32_t b = q & 1u, u = q >> 1;
+    const uint32_t b = q % nstage, u = q / nstage;
     uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
     if (VIS) {
       w0 = n0 >> (8 * quarter);
@@ -246,42 +269,44 @@ __device__ __forceinline__ bool build_tile(const Params& p, const float4* s_tab,
     }
     // the whole warp leaves together (the texel votes below need all 32 lanes)
     if (u > 0 && !__all_sync(0xffffffffu, mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err))) return false;
-    const uint32_t abuf = a_base + b * (3 * 2 * kATile);
-    uint32_t hi[3][4], lo[3][4];
+    const uint32_t abuf = a_base + b * a_stage_bytes(NMAT);
+    const uint32_t off = abuf + (uint32_t)(((row >> 3) * 4 + quarter) * 128 + (row & 7) * 16);
+    // the chunk's 8 texels go out as two 8-byte halves (four texels each), so only two texel pairs'
+    // BF16 parts are held in registers at a time
 #pragma unroll
-    for (int jj = 0; jj < 8; jj += 2) {
-      const int t = st * kStageT + quarter * 8 + jj;
-      const float4 A0 = s_tab[2 * t];
-      const float4 A1 = s_tab[2 * t + 2];
-      const float nl0 = dot3(g.nx, g.ny, g.nz, A0.x, A0.y, A0.z);
-      const float nl1 = dot3(g.nx, g.ny, g.nz, A1.x, A1.y, A1.z);
-      if (!__any_sync(0xffffffffu, nl0 > 0.f || nl1 > 0.f)) {
+    for (int half = 0; half < 2; ++half) {
+      uint32_t hi[NMAT][2], lo[NMAT][2];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) hi[c][jj / 2] = lo[c][jj / 2] = 0u;
-        continue;
+      for (int h = 0; h < 2; ++h) {
+        const int jj = half * 4 + h * 2;
+        const int t = st * kStageT + quarter * 8 + jj;
+        const float4 A0 = s_tab[2 * t];
+        const float4 A1 = s_tab[2 * t + 2];
+        const float nl0 = dot3(g.nx, g.ny, g.nz, A0.x, A0.y, A0.z);
+        const float nl1 = dot3(g.nx, g.ny, g.nz, A1.x, A1.y, A1.z);
+        if (!__any_sync(0xffffffffu, nl0 > 0.f || nl1 > 0.f)) {
+#pragma unroll
+          for (int m = 0; m < NMAT; ++m) hi[m][h] = lo[m][h] = 0u;
+          continue;
+        }
+        const float4 B0 = s_tab[2 * t + 1];
+        const float4 B1 = s_tab[2 * t + 3];
+        const float vis0 = pair_vis<VIS, ONEV>(w0, w1, w2, 1u << jj, g, cs);
+        const float vis1 = pair_vis<VIS, ONEV>(w0, w1, w2, 2u << jj, g, cs);
+        float wd0, ws0, wd1, ws1;
+        pair_fwd_weights<DIFF, SPEC>(g, sc, A0, B0.w, nl0, vis0, wd0, ws0);
+        pair_fwd_weights<DIFF, SPEC>(g, sc, A1, B1.w, nl1, vis1, wd1, ws1);
+        if (DIFF) split2(wd0, wd1, hi[0][h], lo[0][h]);
+        if (SPEC) split2(ws0, ws1, hi[NMAT - 1][h], lo[NMAT - 1][h]);
       }
-      const float4 B0 = s_tab[2 * t + 1];
-      const float4 B1 = s_tab[2 * t + 3];
-      const float vis0 = pair_vis<VIS, ONEV>(w0, w1, w2, 1u << jj, g, cs);
-      const float vis1 = pair_vis<VIS, ONEV>(w0, w1, w2, 2u << jj, g, cs);
-      float wd0, ws0, wd1, ws1;
-      pair_fwd_weights<DIFF, SPEC>(g, sc, A0, B0.w, nl0, vis0, wd0, ws0);
-      pair_fwd_weights<DIFF, SPEC>(g, sc, A1, B1.w, nl1, vis1, wd1, ws1);
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        split2(fmaf(alb[c], wd0, spc[c] * ws0), fmaf(alb[c], wd1, spc[c] * ws1), hi[c][jj / 2], lo[c][jj / 2]);
-    }
-    const uint32_t off = (uint32_t)(((row >> 3) * 4 + quarter) * 128 + (row & 7) * 16);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const uint32_t ahi = abuf + (uint32_t)(c * 2) * kATile + off;
-      asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ahi), "r"(hi[c][0]), "r"(hi[c][1]), "r"(hi[c][2]),
-                   "r"(hi[c][3])
-                   : "memory");
-      if (p.split)
-        asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ahi + kATile), "r"(lo[c][0]), "r"(lo[c][1]),
-                     "r"(lo[c][2]), "r"(lo[c][3])
-                     : "memory");
+      for (int m = 0; m < NMAT; ++m) {
+        const uint32_t ahi = off + (uint32_t)(m * 2) * kATile + half * 8;
+        asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(ahi), "r"(hi[m][0]), "r"(hi[m][1]) : "memory");
+        if (p.split)
+          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(ahi + kATile), "r"(lo[m][0]), "r"(lo[m][1])
+                       : "memory");
+      }
     }
     fence_proxy_async_smem();
     mbar_arrive(&full_a[b]);
@@ -293,39 +318,41 @@ __device__ __forceinline__ bool build_tile(const Params& p, const float4* s_tab,
 
 template <bool DIFF, bool SPEC, bool VIS>
 __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
+  constexpr int NMAT = (DIFF ? 1 : 0) + (SPEC ? 1 : 0);
   extern __shared__ __align__(1024) uint8_t smem[];
   const int HWpad = p.pt.HWpad;
-  const Smem L = smem_layout(HWpad, p.kpad);
+  const Smem L = smem_layout(HWpad, p.kpad, NMAT, p.nstage);
   float4* s_tab = reinterpret_cast<float4*>(smem + L.tab);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar);
-  uint64_t* full_a = bars;          // [2] builders -> MMA
-  uint64_t* full_b = bars + 2;      // [2] producer (tx bytes) -> MMA
-  uint64_t* empty = bars + 4;       // [2] MMA commit -> builders, producer
-  uint64_t* acc_full = bars + 6;    // [2] MMA commit -> epilogue
-  uint64_t* acc_empty = bars + 8;   // [2] epilogue -> MMA
-  uint64_t* drain = bars + 10;      // final MMA drain
+  uint64_t* full_a = bars;          // [nstage] builders -> MMA
+  uint64_t* full_b = bars + 3;      // [nstage] copy warp (tx bytes) -> MMA
+  uint64_t* empty = bars + 6;       // [nstage] MMA commit -> builders, copy warp
+  uint64_t* acc_full = bars + 9;    // [nacc] MMA commit -> epilogue
+  uint64_t* acc_empty = bars + 11;  // [nacc] epilogue -> MMA
+  uint64_t* drain = bars + 13;      // final MMA drain
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + L.misc);
   volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.misc + 8);
   unsigned* err = &p.pt.ctrl[kCtrlError];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t nstage = (uint32_t)p.nstage, nacc = (uint32_t)p.nacc;
   const uint32_t a_base = smem_u32(smem + L.a);
   const uint32_t b_base = smem_u32(smem + L.b);
-  const uint32_t b_tile = (uint32_t)p.kpad * kStageT * 2;
+  const uint32_t b_tile = (uint32_t)p.ncols * kStageT * 2;  // one [ncols x 32] BF16 tile (hi or lo)
   const uint32_t b_stage = bprep_stage_bytes(p.kpad);
+  const uint32_t acc_cols = (uint32_t)(NMAT * p.ncols);     // TMEM columns of one accumulator set
 
   stage_table(s_tab, p.pt.table, 0, HWpad);
   if (threadIdx.x == 0) {
-    mbar_init(&full_a[0], kBuilderThreads);
-    mbar_init(&full_a[1], kBuilderThreads);
-    mbar_init(&full_b[0], 1);
-    mbar_init(&full_b[1], 1);
-    mbar_init(&empty[0], 1);
-    mbar_init(&empty[1], 1);
-    mbar_init(&acc_full[0], 1);
-    mbar_init(&acc_full[1], 1);
-    mbar_init(&acc_empty[0], 128);
-    mbar_init(&acc_empty[1], 128);
+    for (uint32_t i = 0; i < nstage; ++i) {
+      mbar_init(&full_a[i], kBuilderThreads);
+      mbar_init(&full_b[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (uint32_t i = 0; i < nacc; ++i) {
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], 128);
+    }
     mbar_init(drain, 1);
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -353,44 +380,37 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
       const PointGeom g = load_geom<VIS>(p.pt, pid, valid, need_view);
       SpecConst sc;
       if (SPEC) sc = spec_const(valid ? p.pt.rough[pid] : 0.f, g);
-      float alb[3] = {0.f, 0.f, 0.f}, spc[3] = {0.f, 0.f, 0.f};
-      if (valid) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          if (DIFF) alb[c] = p.pt.albedo[3 * pid + c];
-          if (SPEC) spc[c] = p.pt.spec[3 * pid + c];
-        }
-      }
       const bool onev = VIS && warp_single_vertex(g);
-      const bool ok = onev ? build_tile<DIFF, SPEC, VIS, true>(p, s_tab, g, valid, sc, alb, spc, row, quarter, q,
-                                                               a_base, full_a, empty, s_abort, err)
-                           : build_tile<DIFF, SPEC, VIS, false>(p, s_tab, g, valid, sc, alb, spc, row, quarter, q,
-                                                                a_base, full_a, empty, s_abort, err);
+      const bool ok = onev ? build_tile<DIFF, SPEC, VIS, true>(p, s_tab, g, valid, sc, row, quarter, q, a_base, full_a,
+                                                               empty, s_abort, err)
+                           : build_tile<DIFF, SPEC, VIS, false>(p, s_tab, g, valid, sc, row, quarter, q, a_base,
+                                                                full_a, empty, s_abort, err);
       if (!ok) break;
     }
   } else if (warp == kCtrlWarp) {
     // ------------------------------------------------------------------ MMA issue (one thread)
     if (lane == 0) {
-      const uint32_t idesc = umma_idesc_bf16(kTileM, p.kpad);
+      const uint32_t idesc = umma_idesc_bf16(kTileM, p.ncols);
       uint32_t q = 0;
       int i = 0;
       bool ok = true;
       for (int tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x, ++i) {
-        const uint32_t abuf = (uint32_t)i & 1u, au = (uint32_t)i >> 1;
+        const uint32_t abuf = (uint32_t)i % nacc, au = (uint32_t)i / nacc;
         if (au > 0 && !mbar_wait(&acc_empty[abuf], (au - 1) & 1u, s_abort, err)) break;
         tc_fence_after();
         for (int st = 0; st < p.nst; ++st, ++q) {
-          const uint32_t b = q & 1u, u = q >> 1;
+          const uint32_t b = q % nstage, u = q / nstage;
           if (!mbar_wait(&full_a[b], u & 1u, s_abort, err) || !mbar_wait(&full_b[b], u & 1u, s_abort, err)) {
             ok = false;
             break;
           }
           tc_fence_after();
+          const uint32_t bh = b_base + b * b_stage;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const uint32_t d = tmem + (abuf * 3u + (uint32_t)c) * (uint32_t)p.kpad;
-            const uint32_t ah = a_base + b * (3 * 2 * kATile) + (uint32_t)(c * 2) * kATile;
-            const uint32_t bh = b_base + b * b_stage + (uint32_t)(c * 2) * b_tile;
+          for (int m = 0; m < NMAT; ++m) {
+            // D_m[128 x ncols] += W_m[128 x 16] . B[ncols x 16]^T, per 16-texel half of the stage
+            const uint32_t d = tmem + abuf * acc_cols + (uint32_t)m * (uint32_t)p.ncols;
+            const uint32_t ah = a_base + b * a_stage_bytes(NMAT) + (uint32_t)(m * 2) * kATile;
 #pragma unroll
             for (int ks = 0; ks < 2; ++ks) {
               const uint64_t da = umma_desc(ah + ks * 256, 128, 512);
@@ -410,42 +430,60 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
     __syncwarp();
   } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
     // ------------------------------------------------------------------ epilogue
+    // out[p, k, c] = albedo_c D_d[c kpad + k] + specular_c D_s[c kpad + k]
     const uint32_t quarter = (uint32_t)warp & 3u;  // TMEM lanes this warp may access
     const int row = (int)quarter * 32 + lane;
+    const uint32_t lanes = (quarter * 32u) << 16;
     int i = 0;
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++i) {
-      const uint32_t abuf = (uint32_t)i & 1u, au = (uint32_t)i >> 1;
-      if (!mbar_wait(&acc_full[abuf], au & 1u, s_abort, err)) break;
-      tc_fence_after();
+      const uint32_t abuf = (uint32_t)i % nacc, au = (uint32_t)i / nacc;
       int64_t pid = 0;
       const bool live = ordered_point(p.pt.perm, (int64_t)tile * kTileM + row, p.pt.P, p.pt.ctrl, pid);
-      float* orow = p.out + pid * p.ldo + (int64_t)p.kbase * 3;
-      for (int kb = 0; kb < p.kpad / 16; ++kb) {
-        float v[3][16];
+      float alb[3] = {0.f, 0.f, 0.f}, spc[3] = {0.f, 0.f, 0.f};
+      if (live) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-          tmem_ld16(tmem + (quarter * 32u << 16) + (abuf * 3u + (uint32_t)c) * (uint32_t)p.kpad + kb * 16, v[c]);
-        tmem_wait_ld();
+        for (int c = 0; c < 3; ++c) {
+          if (DIFF) alb[c] = p.pt.albedo[3 * pid + c];
+          if (SPEC) spc[c] = p.pt.spec[3 * pid + c];
+        }
+      }
+      if (!mbar_wait(&acc_full[abuf], au & 1u, s_abort, err)) break;
+      tc_fence_after();
+      float* orow = p.out + pid * p.ldo + (int64_t)p.kbase * 3;
+      const uint32_t t0 = tmem + lanes + abuf * acc_cols;
+      for (int kb = 0; kb < p.kpad / 8; ++kb) {
+        float o[3][8];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const uint32_t col = (uint32_t)(c * p.kpad + kb * 8);
+          float v[8];
+          if (DIFF) tmem_ld8(t0 + col, o[c]);
+          if (SPEC) tmem_ld8(t0 + (uint32_t)(NMAT - 1) * (uint32_t)p.ncols + col, v);
+          tmem_wait_ld();
+#pragma unroll
+          for (int e = 0; e < 8; ++e) o[c][e] = DIFF ? (SPEC ? fmaf(spc[c], v[e], alb[c] * o[c][e]) : alb[c] * o[c][e])
+                                                     : spc[c] * v[e];
+        }
         if (live) {
-          const int k0 = kb * 16;
-          if (p.vec_store && k0 + 16 <= p.kblock) {
+          const int k0 = kb * 8;
+          if (p.vec_store && k0 + 8 <= p.kblock) {
             float4* o4 = reinterpret_cast<float4*>(orow + k0 * 3);
 #pragma unroll
-            for (int i4 = 0; i4 < 12; ++i4) {
+            for (int i4 = 0; i4 < 6; ++i4) {
               float x[4];
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
                 const int f = i4 * 4 + e;
-                x[e] = v[f % 3][f / 3];
+                x[e] = o[f % 3][f / 3];
               }
               o4[i4] = make_float4(x[0], x[1], x[2], x[3]);
             }
           } else {
 #pragma unroll
-            for (int kk = 0; kk < 16; ++kk)
+            for (int kk = 0; kk < 8; ++kk)
               if (k0 + kk < p.kblock) {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) orow[(k0 + kk) * 3 + c] = v[c][kk];
+                for (int c = 0; c < 3; ++c) orow[(k0 + kk) * 3 + c] = o[c][kk];
               }
           }
         }
@@ -456,30 +494,27 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
   } else if (warp == kProdWarp) {
     // ------------------------------------------------------------------ radiance bulk copies
     if (lane == 0) {
-      uint32_t q = 0;
-      // copies issued so far into buffer 0 and buffer 1 (the last one into buffer b used phase n_b - 1)
-      uint32_t n_b0 = 0u, n_b1 = 0u;
+      uint32_t q = 0;  // copies issued
       for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
         bool ok = true;
-        for (int st = 0; st < p.nst; ++st, ++q) {
-          const uint32_t b = q & 1u, u = q >> 1;
+        for (int st = 0; st < p.nst; ++st) {
+          const uint32_t b = q % nstage, u = q / nstage;
           if (u > 0 && !mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err)) {
             ok = false;
             break;
           }
           mbar_arrive_expect_tx(&full_b[b], b_stage);
           bulk_g2s(b_base + b * b_stage, p.bprep + (size_t)st * b_stage, b_stage, &full_b[b]);
-          if (b == 0u) ++n_b0;
-          else ++n_b1;
+          ++q;
         }
         if (!ok) break;
       }
       // never leave a bulk copy in flight: wait (bounded) for the last one into each buffer
-      for (int b = 0; b < 2; ++b) {
-        const uint32_t n_issued = b == 0 ? n_b0 : n_b1;
-        if (n_issued == 0u) continue;
+      for (uint32_t b = 0; b < nstage; ++b) {
+        if (q <= b) continue;
+        const uint32_t n_b = (q - b + nstage - 1) / nstage;  // copies into buffer b
         const long long t0 = global_ns();
-        while (!mbar_try_wait(&full_b[b], (n_issued - 1u) & 1u)) {
+        while (!mbar_try_wait(&full_b[b], (n_b - 1u) & 1u)) {
           if (global_ns() - t0 > kWaitNs) {
             atomicOr(err, kErrTimeout);
             break;
@@ -610,14 +645,23 @@ int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigne
 
   RelightFn k = pick_relight(diff, spec, vis);
   const int grid = std::max(1, std::min(prm.ntiles, sms));
+  prm.nmat = (diff ? 1 : 0) + (spec ? 1 : 0);
   for (int kbase = 0; kbase < K; kbase += relight::kEnvBlock) {
     prm.kbase = kbase;
     prm.kblock = std::min(relight::kEnvBlock, K - kbase);
     prm.kpad = kpad_of(prm.kblock);
+    prm.ncols = 3 * prm.kpad;
+    // two accumulator sets (the epilogue of one tile overlaps the MMAs of the next) when they fit
+    // in the 512 TMEM columns, else one
+    prm.nacc = 2 * prm.nmat * prm.ncols <= (int)relight::kTmemCols ? 2 : 1;
     prm.vec_store = ((reinterpret_cast<uintptr_t>(out) & 15u) == 0) && (prm.ldo % 4 == 0) && ((kbase * 3) % 4 == 0);
-    const relight::Smem L = relight::smem_layout(HWpad, prm.kpad);
+    // the deepest ring that fits in shared memory
+    prm.nstage = relight::kMaxStages;
+    while (prm.nstage > 2 && (int)relight::smem_layout(HWpad, prm.kpad, prm.nmat, prm.nstage).total > max_smem)
+      --prm.nstage;
+    const relight::Smem L = relight::smem_layout(HWpad, prm.kpad, prm.nmat, prm.nstage);
     if ((int)L.total > max_smem) return DES_ERR_UNSUPPORTED;
-    const int total = prm.nst * 3 * prm.kpad * relight::kStageT;
+    const int total = prm.nst * prm.ncols * relight::kStageT;
     relight::prep_kernel<<<(total + 255) / 256, 256, 0, stream>>>(envmaps, HW, prm.nst, kbase, prm.kblock, prm.kpad,
                                                                   bprep);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;

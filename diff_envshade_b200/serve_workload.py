@@ -283,6 +283,7 @@ if __name__ == "__main__":
     ap.add_argument("--n", type=int, default=2000)
     ap.add_argument("--rate", type=float, default=5000.0)
     ap.add_argument("--tick-us", type=int, default=75)
+    ap.add_argument("--seed", type=int, default=7, help="seed of the arrival schedule")
     ap.add_argument("--ticks-in-flight", type=int, default=None)
     ap.add_argument("--no-serial", action="store_true")
     ap.add_argument("--single", type=int, default=0, help="time one request of this many points instead")
@@ -298,4 +299,4 @@ if __name__ == "__main__":
                                     order_min_points=a.order_min_points)))
     else:
         print(json.dumps(run(n=a.n, rate=a.rate, tick_us=a.tick_us, serial=not a.no_serial,
-                             ticks_in_flight=a.ticks_in_flight)))
+                             ticks_in_flight=a.ticks_in_flight, seed=a.seed)))
