@@ -533,21 +533,24 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
 }
 
 // Deterministic FP64 sum of the per-CTA env-gradient partials: g_env[c][t] = sum_b partial[b][c][t].
-// Block = 32 columns x 32 rows; rows stride over the partials, then a fixed-order tree over rows.
-__global__ void __launch_bounds__(1024) des_env_reduce_kernel(const double* __restrict__ partial, int nparts,
-                                                              int HW, int HWpad, float* __restrict__ g_env) {
-  __shared__ double s[32][33];
+// Block = kReduceCols columns x kReduceRows rows (192 blocks for a 16x32 map, so every SM takes part):
+// row y sums partials y, y + kReduceRows, ... in order, then a fixed-order tree over the rows.
+constexpr int kReduceCols = 8, kReduceRows = 128;
+__global__ void __launch_bounds__(kReduceCols* kReduceRows) des_env_reduce_kernel(const double* __restrict__ partial,
+                                                                                  int nparts, int HW, int HWpad,
+                                                                                  float* __restrict__ g_env) {
+  __shared__ double s[kReduceRows][kReduceCols + 1];
   const int x = threadIdx.x, y = threadIdx.y;
-  const int k = blockIdx.x * 32 + x;  // index into [3][HWpad]
+  const int k = blockIdx.x * kReduceCols + x;  // index into [3][HWpad]
   const int n = 3 * HWpad;
   double acc = 0.0;
   if (k < n) {
-    for (int b = y; b < nparts; b += 32) acc += partial[(size_t)b * n + k];
+    for (int b = y; b < nparts; b += kReduceRows) acc += partial[(size_t)b * n + k];
   }
   s[y][x] = acc;
   __syncthreads();
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
+  for (int off = kReduceRows / 2; off > 0; off >>= 1) {
     if (y < off) s[y][x] += s[y + off][x];
     __syncthreads();
   }
@@ -874,8 +877,8 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   if (ev0 != nullptr && ev1 != nullptr) cudaEventRecord(ev1, stream);
 
   if (call.backward && call.g_envmap != nullptr) {
-    const dim3 rb(32, 32);
-    const int rg = (3 * lp.HWpad + 31) / 32;
+    const dim3 rb(kReduceCols, kReduceRows);
+    const int rg = (3 * lp.HWpad + kReduceCols - 1) / kReduceCols;
     des_env_reduce_kernel<<<rg, rb, 0, stream>>>(env_partial, grid, a.H * a.W, lp.HWpad, call.g_envmap);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
     count_launches(1);
