@@ -231,12 +231,16 @@ __device__ __forceinline__ void fwd_tile_slots(const ReqDesc& r, const PointGeom
   const float cs = (g.c0 + g.c1) + g.c2;
   const int nsl = r.HWpad >> 5;
   const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
-  for (int k = 0;; ++k) {
-    const int cur = warp_slot(k, warp, kNW, nsl, ushift);
-    if (cur < 0) break;
-    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
+  // the visibility words of a warp's next slot are loaded while it integrates the current one
+  uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
+  int sl = warp_slot(0, warp, kNW, nsl, ushift);
+  if (VIS && sl >= 0) load_vis_words<ONEV>(r, g, valid, sl, n0, n1, n2);
+  for (int k = 1; sl >= 0; ++k) {
+    const int cur = sl;
+    sl = warp_slot(k, warp, kNW, nsl, ushift);
+    const uint32_t w0 = n0, w1 = n1, w2 = n2;
     if (VIS) {
-      load_vis_words<ONEV>(r, g, valid, cur, w0, w1, w2);
+      if (sl >= 0) load_vis_words<ONEV>(r, g, valid, sl, n0, n1, n2);
       if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
     }
     fwd_slot<DIFF, SPEC, VIS, ONEV>(g, sc, cs, s_tab + 2 * (cur << 5), w0, w1, w2, acc);
@@ -253,12 +257,15 @@ __device__ __forceinline__ void bwd_tile_slots(const ReqDesc& r, const PointGeom
   const int nsl = r.HWpad >> 5;
   const int ushift = ((nsl + 1) >> 1) >= kNW ? 1 : 0;
   const int jsel = butterfly_texel(lane);
-  for (int k = 0;; ++k) {
-    const int cur = warp_slot(k, warp, kNW, nsl, ushift);
-    if (cur < 0) break;
-    uint32_t w0 = 0u, w1 = 0u, w2 = 0u;
+  uint32_t n0 = 0u, n1 = 0u, n2 = 0u;
+  int sl = warp_slot(0, warp, kNW, nsl, ushift);
+  if (VIS && sl >= 0) load_vis_words<ONEV>(r, g, valid, sl, n0, n1, n2);
+  for (int k = 1; sl >= 0; ++k) {
+    const int cur = sl;
+    sl = warp_slot(k, warp, kNW, nsl, ushift);
+    const uint32_t w0 = n0, w1 = n1, w2 = n2;
     if (VIS) {
-      load_vis_words<ONEV>(r, g, valid, cur, w0, w1, w2);
+      if (sl >= 0) load_vis_words<ONEV>(r, g, valid, sl, n0, n1, n2);
       if (!__any_sync(0xffffffffu, (w0 | w1 | w2) != 0u)) continue;
     }
     const int t0 = (cur << 5) + jsel;
