@@ -93,3 +93,24 @@ def test_no_points(des):
     assert g[5].shape == d.envmap.shape
     assert_close_grad(g[5].cpu(), torch.zeros(d.envmap.shape), "empty:g_envmap")
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("P", [1000, 20000], ids=["input-order", "ordered"])
+def test_single_vertex_path_matches_three_word_path(des, P):
+    """A warp whose points each use one visibility row (triangle (p, p, p), barycentrics (1, 0, 0))
+    takes the one-word visibility path.  Giving point 0 a genuine three-vertex triangle with the same
+    barycentrics (1, 0, 0) keeps every visibility value the same but sends its warp down the general
+    three-word path: every output must stay the same bit for bit."""
+    from diff_envshade_b200 import workloads as wl
+    inp = wl.make_inputs(P, 16, 32, seed=77, vis_p=0.7, vis_layout="identity", rotation=True)
+    d = inp.to("cuda")
+    alt = inp.to("cuda")
+    extra = torch.tensor([[0], [1], [2]], dtype=torch.int32, device="cuda")
+    alt.face_vertex_list = torch.cat([d.face_vertex_list, extra], dim=1).contiguous()
+    tri = d.nearest_triangle_id.clone()
+    tri[0] = P  # the appended face (0, 1, 2)
+    alt.nearest_triangle_id = tri
+    got = run_op(des, "specularvisibility2", d)
+    ref = run_op(des, "specularvisibility2", alt)
+    for k in got:
+        assert torch.equal(got[k], ref[k]), k
