@@ -452,18 +452,20 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
       float* orow = p.out + pid * p.ldo + (int64_t)p.kbase * 3;
       const uint32_t t0 = tmem + lanes + abuf * acc_cols;
       for (int kb = 0; kb < p.kpad / 8; ++kb) {
-        float o[3][8];
+        // all six 8-column loads of the chunk (both terms, three channels) in flight before one wait
+        float o[3][8], v[3][8];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const uint32_t col = (uint32_t)(c * p.kpad + kb * 8);
-          float v[8];
           if (DIFF) tmem_ld8(t0 + col, o[c]);
-          if (SPEC) tmem_ld8(t0 + (uint32_t)(NMAT - 1) * (uint32_t)p.ncols + col, v);
-          tmem_wait_ld();
-#pragma unroll
-          for (int e = 0; e < 8; ++e) o[c][e] = DIFF ? (SPEC ? fmaf(spc[c], v[e], alb[c] * o[c][e]) : alb[c] * o[c][e])
-                                                     : spc[c] * v[e];
+          if (SPEC) tmem_ld8(t0 + (uint32_t)(NMAT - 1) * (uint32_t)p.ncols + col, v[c]);
         }
+        tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            o[c][e] = DIFF ? (SPEC ? fmaf(spc[c], v[c][e], alb[c] * o[c][e]) : alb[c] * o[c][e]) : spc[c] * v[c][e];
         if (live) {
           const int k0 = kb * 8;
           if (p.vec_store && k0 + 8 <= p.kblock) {
