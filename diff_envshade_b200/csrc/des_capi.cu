@@ -19,7 +19,8 @@ int validate(const des_shade_args* a, unsigned flags, bool backward, const void*
   if (a->C != 3) return DES_ERR_UNSUPPORTED;
   if (a->P < 0 || a->H <= 0 || a->W <= 0) return DES_ERR_INVALID_ARGUMENT;
   if ((int64_t)a->H * a->W > kMaxTexels) return DES_ERR_UNSUPPORTED;
-  if (flags & ~(unsigned)(DES_DIFFUSE | DES_SPECULAR | DES_CLAMP | DES_INPUT_ORDER | DES_COMPACT | DES_REUSE_ORDER))
+  if (flags & ~(unsigned)(DES_DIFFUSE | DES_SPECULAR | DES_CLAMP | DES_INPUT_ORDER | DES_COMPACT | DES_REUSE_ORDER |
+                          DES_REUSE_TABLE))
     return DES_ERR_INVALID_ARGUMENT;
   if (a->envmap == nullptr || a->light2obj_rotmat == nullptr) return DES_ERR_INVALID_ARGUMENT;
   if (a->P == 0) return DES_OK;

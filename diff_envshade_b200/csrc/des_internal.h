@@ -26,7 +26,10 @@ inline int sort_chunk_for(int64_t P) {
 }
 
 // control words at the start of every workspace
-enum : int { kCtrlTileCounter = 0, kCtrlError = 1 };
+// (the forward and the adjoint claim tiles from separate counters, so an adjoint that reuses the
+// texel table of the forward before it -- DES_REUSE_TABLE -- needs no kernel to reset its counter;
+// every table or ordering kernel resets all three words)
+enum : int { kCtrlTileCounter = 0, kCtrlError = 1, kCtrlTileCounterBwd = 2 };
 
 // Kernel parameters (passed by value in the launch).
 struct ShadeParams {

@@ -19,7 +19,7 @@
 //    the tile counter and error word and overwrites the texel table and every env-gradient partial it
 //    reads, so nothing left over is ever used -- but two calls whose work overlaps on the GPU (other
 //    streams, other host threads) race on the array and corrupt each other's results;
-//  * DES_REUSE_ORDER is ignored here: no forward ever leaves its point ordering in this array, so a
+//  * DES_REUSE_ORDER and DES_REUSE_TABLE are ignored here: no forward ever leaves its state in this array, so a
 //    call that ordered its points always computes the ordering itself (a permutation left over from
 //    an earlier call of another size would drop points);
 //  * errors found on the device (out-of-range triangle or vertex ids, which des_workspace_status
@@ -67,7 +67,7 @@ extern "C" int des_shade_backward_noalloc(const des_shade_args* args, unsigned f
                                           float* g_albedo, float* g_specular_albedo, float* g_roughness,
                                           float* g_envmap, des_stream_t stream) {
   if (args == nullptr) return DES_ERR_INVALID_ARGUMENT;
-  flags &= ~(unsigned)DES_REUSE_ORDER;  // the array never holds a forward's ordering
+  flags &= ~(unsigned)(DES_REUSE_ORDER | DES_REUSE_TABLE);  // the array never holds a forward's state
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return DES_ERR_CUDA;
   const size_t need = des_shade_workspace_bytes(args->P, args->H, args->W, flags | DES_COMPACT, 1, dev);

@@ -86,6 +86,7 @@ __global__ void des_table_kernel(int H, int W, int HWpad, const float* __restric
   if (t == 0 && ctrl != nullptr) {
     ctrl[kCtrlTileCounter] = 0u;
     ctrl[kCtrlError] = 0u;
+    ctrl[kCtrlTileCounterBwd] = 0u;
   }
   if (t < HWpad) table_entry(t, H, W, R, env, rec, export4);
 }
@@ -152,6 +153,7 @@ __global__ void __launch_bounds__(kSortThreads, 1) des_prep_kernel(int H, int W,
   if (blockIdx.x == 0 && tid == 0 && ctrl != nullptr) {
     ctrl[kCtrlTileCounter] = 0u;
     ctrl[kCtrlError] = 0u;
+    ctrl[kCtrlTileCounterBwd] = 0u;
   }
   for (int t = blockIdx.x * kSortThreads + tid; t < HWpad; t += gridDim.x * kSortThreads)
     table_entry(t, H, W, R, env, rec, nullptr);
@@ -466,7 +468,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadePara
   int tile = blockIdx.x;
   int it = 0;
   while (tile < p.ntiles) {
-    if (threadIdx.x == 0) s_next[it & 1] = (int)gridDim.x + (int)atomicAdd(&p.ctrl[kCtrlTileCounter], 1u);
+    if (threadIdx.x == 0) s_next[it & 1] = (int)gridDim.x + (int)atomicAdd(&p.ctrl[kCtrlTileCounterBwd], 1u);
 
     const int64_t slot = (int64_t)tile * 32 + lane;
     int64_t pid = slot;
@@ -793,7 +795,12 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   // already holds this problem's ordering from the previous call on it)
   const bool sort = lp.sort && a.P > 0 && (diff || spec);
   const bool reuse = sort && (call.flags & DES_REUSE_ORDER) != 0;
-  if (sort && !reuse) {
+  // an adjoint right after its forward on this workspace: the table (and the ordering, when the
+  // call orders its points and reuses it) are there already, and its tile counter is still zero
+  const bool reuse_table = call.backward && (call.flags & DES_REUSE_TABLE) != 0 && (!sort || reuse);
+  if (reuse_table) {
+    // nothing to launch before the adjoint
+  } else if (sort && !reuse) {
     des_prep_kernel<<<lp.sort_chunks, kSortThreads, 0, stream>>>(a.H, a.W, lp.HWpad, a.light2obj_rotmat, a.envmap,
                                                                  table, ctrl, a.normal, a.P, lp.sort_chunk,
                                                                  sort_row(lp), sort_counts, sort_keys, sort_rank);
@@ -804,7 +811,7 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
                                                      nullptr, ctrl);
   }
   if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
-  count_launches(1);
+  if (!reuse_table) count_launches(1);
   if (a.P == 0) {
     if (call.backward && call.g_envmap != nullptr)
       if (cudaMemsetAsync(call.g_envmap, 0, sizeof(float) * 3 * (size_t)a.H * a.W, stream) != cudaSuccess)

@@ -138,29 +138,48 @@ des_stream_t cur_stream_h() { return reinterpret_cast<des_stream_t>(at::cuda::ge
 // the forward and the adjoint of a problem).  When a call passes the same points as the previous
 // successful call on it -- the same normal tensor storage, offset, point count and version, and
 // the same map size -- the workspace still holds their normal-direction ordering and the call skips
-// recomputing it (DES_REUSE_ORDER): the adjoint after its forward, the usual pattern.  A call on
-// another stream gets a fresh buffer (never one that another stream may still be using).  The entry
-// holds a reference to the normals' storage, so that storage cannot be freed and its address reused
-// by other points while the entry exists (the most recent normals stay allocated until the next call).
+// recomputing it (DES_REUSE_ORDER): the adjoint after its forward, the usual pattern.  When that
+// previous call was the forward and the env map and rotation are the same tensors at the same
+// versions too, the adjoint also reuses the forward's texel table (DES_REUSE_TABLE) and launches no
+// kernel before its own.  A call on another stream gets a fresh buffer (never one that another
+// stream may still be using).  The entry holds references to the storages it compares, so they
+// cannot be freed and their addresses reused by other tensors while the entry exists (the most
+// recent inputs stay allocated until the next call).
+struct TensorKey {
+  c10::Storage storage;
+  int64_t offset = -1;
+  uint32_t version = 0;
+  void set(const Tensor& t) {
+    storage = t.storage();
+    offset = t.storage_offset();
+    version = t._version();
+  }
+  bool same(const Tensor& t) const {
+    return storage.unsafeGetStorageImpl() == t.storage().unsafeGetStorageImpl() && offset == t.storage_offset() &&
+           version == t._version();
+  }
+};
+
 struct WsEntry {
   Tensor ws;
   cudaStream_t stream = nullptr;
-  c10::Storage storage;
-  int64_t offset = -1, P = -1;
-  uint32_t version = 0;
+  TensorKey normal, envmap, rot;
+  int64_t P = -1;
   int H = 0, W = 0;
   bool holds_order = false;
+  bool after_forward = false;  // the last successful call was a forward
 };
 std::mutex g_ws_mu;
 WsEntry g_ws[64];
 
 struct WsLease {
   Tensor ws;
-  unsigned extra = 0;  // DES_REUSE_ORDER when the workspace holds these points' ordering
+  unsigned extra = 0;  // DES_REUSE_ORDER / DES_REUSE_TABLE when the workspace holds that state
   int dev = 0;
 };
 
-WsLease lease_workspace(const Tensor& normal, const Common& c, unsigned flags) {
+WsLease lease_workspace(const Tensor& normal, const Tensor& envmap, const Tensor& R, const Common& c, unsigned flags,
+                        bool backward) {
   WsLease L;
   L.dev = normal.get_device();
   TORCH_CHECK(L.dev >= 0 && L.dev < 64, "diff_envshade_b200: device index out of range");
@@ -175,27 +194,29 @@ WsLease lease_workspace(const Tensor& normal, const Common& c, unsigned flags) {
     e.ws = torch::empty({(int64_t)need}, normal.options().dtype(torch::kUInt8));
     e.stream = stream;
   }
-  const bool same = e.holds_order && e.storage.unsafeGetStorageImpl() == normal.storage().unsafeGetStorageImpl() &&
-                    e.offset == normal.storage_offset() && e.P == c.P && e.version == normal._version() &&
-                    e.H == c.H && e.W == c.W;
+  const bool same = e.holds_order && e.normal.same(normal) && e.P == c.P && e.H == c.H && e.W == c.W;
   L.ws = e.ws;
   L.extra = same ? DES_REUSE_ORDER : 0u;
+  if (same && backward && e.after_forward && e.envmap.same(envmap) && e.rot.same(R)) L.extra |= DES_REUSE_TABLE;
   e.holds_order = false;  // until this call has succeeded
+  e.after_forward = false;
   return L;
 }
 
-// After a successful call: the workspace now holds the ordering of these points.
-void workspace_done(const WsLease& L, const Tensor& normal, const Common& c) {
+// After a successful call: the workspace now holds the ordering (and texel table) of these inputs.
+void workspace_done(const WsLease& L, const Tensor& normal, const Tensor& envmap, const Tensor& R, const Common& c,
+                    bool backward) {
   std::lock_guard<std::mutex> lk(g_ws_mu);
   WsEntry& e = g_ws[L.dev];
   if (!e.ws.defined() || !e.ws.is_same(L.ws)) return;
-  e.storage = normal.storage();
-  e.offset = normal.storage_offset();
+  e.normal.set(normal);
+  e.envmap.set(envmap);
+  e.rot.set(R);
   e.P = c.P;
-  e.version = normal._version();
   e.H = c.H;
   e.W = c.W;
   e.holds_order = true;
+  e.after_forward = !backward;
 }
 
 des_shade_args make_args(const Common& c, const Tensor& normal, const Tensor* view, const Tensor& albedo,
@@ -227,25 +248,26 @@ void add_visibility(des_shade_args& a, const VisArgs& v, const Tensor& faces, co
 }
 
 // The forward / adjoint of one operator through the shared workspace.
-int run_forward(const des_shade_args& a, const Tensor& normal, const Common& c, unsigned flags, Tensor& shading,
-                Tensor* white) {
-  WsLease L = lease_workspace(normal, c, flags);
+int run_forward(const des_shade_args& a, const Tensor& normal, const Tensor& envmap, const Tensor& R, const Common& c,
+                unsigned flags, Tensor& shading, Tensor* white) {
+  WsLease L = lease_workspace(normal, envmap, R, c, flags, false);
   const int st = des_shade_forward(&a, flags | L.extra, shading.data_ptr<float>(),
                                    white ? white->data_ptr<float>() : nullptr, L.ws.data_ptr(), (size_t)L.ws.numel(),
                                    cur_stream_h());
-  if (st == DES_OK) workspace_done(L, normal, c);
+  if (st == DES_OK) workspace_done(L, normal, envmap, R, c, false);
   finish(st, L.ws, at::cuda::getCurrentCUDAStream().stream());
   return st;
 }
 
-int run_backward(const des_shade_args& a, const Tensor& normal, const Common& c, unsigned flags, const Tensor& gsh,
-                 const Tensor* gwh, Tensor& gn, Tensor* gv, Tensor& ga, Tensor* gs, Tensor* gr, Tensor& genv) {
-  WsLease L = lease_workspace(normal, c, flags);
+int run_backward(const des_shade_args& a, const Tensor& normal, const Tensor& envmap, const Tensor& R, const Common& c,
+                 unsigned flags, const Tensor& gsh, const Tensor* gwh, Tensor& gn, Tensor* gv, Tensor& ga, Tensor* gs,
+                 Tensor* gr, Tensor& genv) {
+  WsLease L = lease_workspace(normal, envmap, R, c, flags, true);
   const int st = des_shade_backward(&a, flags | L.extra, gsh.data_ptr<float>(), gwh ? gwh->data_ptr<float>() : nullptr,
                                     gn.data_ptr<float>(), gv ? gv->data_ptr<float>() : nullptr, ga.data_ptr<float>(),
                                     gs ? gs->data_ptr<float>() : nullptr, gr ? gr->data_ptr<float>() : nullptr,
                                     genv.data_ptr<float>(), L.ws.data_ptr(), (size_t)L.ws.numel(), cur_stream_h());
-  if (st == DES_OK) workspace_done(L, normal, c);
+  if (st == DES_OK) workspace_done(L, normal, envmap, R, c, true);
   finish(st, L.ws, at::cuda::getCurrentCUDAStream().stream());
   return st;
 }
@@ -266,7 +288,7 @@ Tensor bruteforce_diffuse_shader_forward(const Tensor& normal, const Tensor& alb
   auto opt = normal.options().requires_grad(false);
   Tensor shading = torch::empty({c.P, c.C}, opt);
   const des_shade_args a = make_args(c, normal, nullptr, albedo, nullptr, nullptr, envmap, R);
-  run_forward(a, normal, c, DES_DIFFUSE, shading, nullptr);
+  run_forward(a, normal, envmap, R, c, DES_DIFFUSE, shading, nullptr);
   return shading;
 }
 
@@ -281,7 +303,7 @@ std::vector<Tensor> bruteforce_diffuse_shader_backward(const Tensor& grad_shadin
   Tensor g_normal = torch::empty({c.P, 3}, opt);
   Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
   const des_shade_args a = make_args(c, normal, nullptr, albedo, nullptr, nullptr, envmap, R);
-  run_backward(a, normal, c, DES_DIFFUSE, grad_shading, nullptr, g_normal, nullptr, g_albedo, nullptr, nullptr, g_env);
+  run_backward(a, normal, envmap, R, c, DES_DIFFUSE, grad_shading, nullptr, g_normal, nullptr, g_albedo, nullptr, nullptr, g_env);
   return {g_normal, g_albedo, g_env};
 }
 
@@ -295,7 +317,7 @@ Tensor specular_forward_impl(const Tensor& normal, const Tensor& view, const Ten
   Tensor shading = torch::empty({c.P, c.C}, opt);
   unsigned f = (enable_diffuse ? DES_DIFFUSE : 0u) | (enable_specular ? DES_SPECULAR : 0u) | (clamp ? DES_CLAMP : 0u);
   const des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
-  run_forward(a, normal, c, f, shading, nullptr);
+  run_forward(a, normal, envmap, R, c, f, shading, nullptr);
   return shading;
 }
 
@@ -317,7 +339,7 @@ std::vector<Tensor> specular_backward_impl(const Tensor& grad_shading, const Ten
   Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
   unsigned f = (enable_diffuse ? DES_DIFFUSE : 0u) | (enable_specular ? DES_SPECULAR : 0u) | (clamp ? DES_CLAMP : 0u);
   const des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
-  run_backward(a, normal, c, f, grad_shading, nullptr, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
+  run_backward(a, normal, envmap, R, c, f, grad_shading, nullptr, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
   return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
 }
 
@@ -360,7 +382,7 @@ std::vector<Tensor> bruteforce_specular_shader_forward2(const Tensor& normal, co
   Tensor white = torch::empty({c.P, c.C}, opt);
   unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
   const des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
-  run_forward(a, normal, c, f, shading, &white);
+  run_forward(a, normal, envmap, R, c, f, shading, &white);
   return {shading, white};
 }
 
@@ -385,7 +407,7 @@ std::vector<Tensor> bruteforce_specular_shader_backward2(const Tensor& grad_shad
   Tensor g_env = torch::empty({c.C, c.H, c.W}, opt);
   unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
   const des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
-  run_backward(a, normal, c, f, grad_shading, &grad_white, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
+  run_backward(a, normal, envmap, R, c, f, grad_shading, &grad_white, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
   return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
 }
 
@@ -403,7 +425,7 @@ std::vector<Tensor> bruteforce_specularvisibility_shader_forward2(
   unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
   des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
   add_visibility(a, v, faces, tri, bary, vis);
-  run_forward(a, normal, c, f, shading, &white);
+  run_forward(a, normal, envmap, R, c, f, shading, &white);
   return {shading, white};
 }
 
@@ -429,7 +451,7 @@ std::vector<Tensor> bruteforce_specularvisibility_shader_backward2(
   unsigned f = DES_DIFFUSE | (enable_specular ? DES_SPECULAR : 0u);
   des_shade_args a = make_args(c, normal, &view, albedo, &spec, &rough, envmap, R);
   add_visibility(a, v, faces, tri, bary, vis);
-  run_backward(a, normal, c, f, grad_shading, &grad_white, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
+  run_backward(a, normal, envmap, R, c, f, grad_shading, &grad_white, g_normal, &g_view, g_albedo, &g_spec, &g_rough, g_env);
   return {g_normal, g_view, g_albedo, g_spec, g_rough, g_env};
 }
 

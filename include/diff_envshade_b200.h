@@ -65,6 +65,13 @@ typedef enum des_status {
  * bit for bit and the env-map gradient differs only in FP64 summation order.  Ignored for calls
  * that do not order their points. */
 #define DES_REUSE_ORDER 64u
+/* des_shade_backward: the call immediately before this one on the same workspace was the forward
+ * of the same problem (same env map and rotation, and for an ordered call the same normals, with
+ * DES_REUSE_ORDER also passed): its texel table is reused and the adjoint launches no table or
+ * ordering kernel first.  Only the caller can know this; the table kernel's reset of the error word
+ * is skipped too, so des_workspace_status then reports the forward's and the adjoint's errors
+ * together.  Ignored by des_shade_forward. */
+#define DES_REUSE_TABLE 128u
 
 /* All inputs of one shading call.  The visibility block is ignored when visibility == NULL. */
 typedef struct des_shade_args {
@@ -127,7 +134,7 @@ int des_shade_backward(const des_shade_args* args, unsigned flags, const float* 
  * (a problem that fits only a smaller plan runs with that plan, see DES_COMPACT).  All calls share the
  * array: calls whose work overlaps on the GPU race and corrupt each other.  The first call on each
  * device looks up the array's address (cudaGetSymbolAddress); make it before any stream capture.
- * DES_REUSE_ORDER is ignored (the array never holds a forward's ordering).  Out-of-range mesh ids
+ * DES_REUSE_ORDER and DES_REUSE_TABLE are ignored (the array never holds a forward's state).  Out-of-range mesh ids
  * found on the device shade to zero but are not reported (there is no caller-visible workspace for
  * des_workspace_status to read).  Allocates nothing. */
 int des_shade_backward_noalloc(const des_shade_args* args, unsigned flags, const float* grad_shading,

@@ -16,6 +16,7 @@ DES_DIFFUSE, DES_SPECULAR, DES_CLAMP = 1, 2, 4
 DES_INPUT_ORDER = 16
 DES_COMPACT = 32
 DES_REUSE_ORDER = 64
+DES_REUSE_TABLE = 128
 
 vp = ctypes.c_void_p
 
