@@ -357,8 +357,9 @@ def test_point_ordering_changes_no_result(des, P, layout):
 
 def test_backward_reuses_its_forwards_ordering(des):
     """The torch ops keep one workspace per device: a backward that follows its forward on the same
-    normals skips the two ordering kernels (3 launches instead of 4); modifying the normals (their
-    version counter) makes the next call order the points again."""
+    normals, env map and rotation skips the ordering and texel-table kernels (2 launches instead of
+    4); modifying the normals (their version counter) makes the next call order the points again, and
+    a backward after a backward rebuilds the table."""
     from diff_envshade_b200 import workloads as wl
     d = _dev(wl.make_inputs(70000, 16, 32, seed=91, vis_p=0.7, rotation=True))
     base = (d.normal, d.view_dir, d.albedo, d.specular_albedo, d.roughness, d.envmap, d.light2obj_rotmat)
@@ -369,7 +370,7 @@ def test_backward_reuses_its_forwards_ordering(des):
     n1 = des.kernel_launches()
     g = des.bruteforce_specularvisibility_shader_backward2(gs, gw, *base, *vis, True)
     n2 = des.kernel_launches()
-    assert n1 - n0 == 3 and n2 - n1 == 3, (n1 - n0, n2 - n1)  # fwd: prep, place, shade; bwd: table, shade, reduce
+    assert n1 - n0 == 3 and n2 - n1 == 2, (n1 - n0, n2 - n1)  # fwd: prep, place, shade; bwd: shade, reduce
     torch.autograd.graph.increment_version(d.normal)
     g2 = des.bruteforce_specularvisibility_shader_backward2(gs, gw, *base, *vis, True)
     n3 = des.kernel_launches()
