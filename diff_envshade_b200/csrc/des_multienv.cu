@@ -68,7 +68,8 @@ struct Params {
   int nmat;               // weight matrices per stage: Lambert and/or GGX (1 or 2)
   int nstage;             // ring depth (2 or 3)
   int nacc;               // TMEM accumulator sets (2 when 2 * nmat * ncols columns fit, else 1)
-  bool split, vec_store;
+  bool split;
+  int vec;                // output row chunks stored as 32-byte (2), 16-byte (1) or scalar (0) writes
 };
 
 struct Smem {  // byte offsets into dynamic shared memory
@@ -191,6 +192,12 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
                : "r"(taddr));
 #pragma unroll
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+// 32-byte global store (sm_100: st.global.v8.f32); the address is 32-byte aligned.
+__device__ __forceinline__ void st_global_v8(float* ptr, const float (&x)[8]) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(ptr), "f"(x[0]), "f"(x[1]), "f"(x[2]),
+               "f"(x[3]), "f"(x[4]), "f"(x[5]), "f"(x[6]), "f"(x[7])
+               : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -468,7 +475,21 @@ __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
             o[c][e] = DIFF ? (SPEC ? fmaf(spc[c], v[c][e], alb[c] * o[c][e]) : alb[c] * o[c][e]) : spc[c] * v[c][e];
         if (live) {
           const int k0 = kb * 8;
-          if (p.vec_store && k0 + 8 <= p.kblock) {
+          if (p.vec == 2 && k0 + 8 <= p.kblock) {
+            // a chunk's 24 outputs (8 maps x 3 channels, contiguous in the row) as three 32-byte
+            // stores: each writes whole 32-byte sectors, half the store instructions of float4s
+            float* o8 = orow + k0 * 3;
+#pragma unroll
+            for (int i8 = 0; i8 < 3; ++i8) {
+              float x[8];
+#pragma unroll
+              for (int e = 0; e < 8; ++e) {
+                const int f = i8 * 8 + e;
+                x[e] = o[f % 3][f / 3];
+              }
+              st_global_v8(o8 + i8 * 8, x);
+            }
+          } else if (p.vec == 1 && k0 + 8 <= p.kblock) {
             float4* o4 = reinterpret_cast<float4*>(orow + k0 * 3);
 #pragma unroll
             for (int i4 = 0; i4 < 6; ++i4) {
@@ -656,7 +677,10 @@ int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigne
     // two accumulator sets (the epilogue of one tile overlaps the MMAs of the next) when they fit
     // in the 512 TMEM columns, else one
     prm.nacc = 2 * prm.nmat * prm.ncols <= (int)relight::kTmemCols ? 2 : 1;
-    prm.vec_store = ((reinterpret_cast<uintptr_t>(out) & 15u) == 0) && (prm.ldo % 4 == 0) && ((kbase * 3) % 4 == 0);
+    const uintptr_t oa = reinterpret_cast<uintptr_t>(out);
+    prm.vec = ((oa & 31u) == 0 && prm.ldo % 8 == 0 && (kbase * 3) % 8 == 0)   ? 2
+              : ((oa & 15u) == 0 && prm.ldo % 4 == 0 && (kbase * 3) % 4 == 0) ? 1
+                                                                               : 0;
     // the deepest ring that fits in shared memory
     prm.nstage = relight::kMaxStages;
     while (prm.nstage > 2 && (int)relight::smem_layout(HWpad, prm.kpad, prm.nmat, prm.nstage).total > max_smem)
