@@ -251,9 +251,9 @@ __global__ void prep_kernel(const float* __restrict__ env, int HW, int nst, int 
 // point row `row` of the weight matrices -- W_d = the Lambert weight wd and W_s = the GGX weight ws
 // (whichever of the two terms is on), as BF16 hi and lo parts -- into the stage's shared-memory A
 // tiles (K-major canonical layout).  The albedos are applied per point in the epilogue, so one pair
-// of matrices serves all three colour channels.  Texels are taken in pairs: a pair below the horizon
-// of the warp's 32 (ordered) points gets zero weights after one vote, otherwise both are evaluated
-// side by side.  The visibility words of the next stage are loaded while this one is built.  q counts
+// of matrices serves all three colour channels.  Texels are taken in fours: four texels below the
+// horizon of the warp's 32 (ordered) points get zero weights after one vote, otherwise all four are
+// evaluated side by side.  The visibility words of the next stage are loaded while this one is built.  q counts
 // the stages this thread has filled (ring position).  Returns false when the CTA gave up waiting (the
 // whole warp leaves together).
 template <bool DIFF, bool SPEC, bool VIS, bool ONEV>
@@ -278,33 +278,36 @@ __device__ __forceinline__ bool build_tile(const Params& p, const float4* s_tab,
     if (u > 0 && !__all_sync(0xffffffffu, mbar_wait(&empty[b], (u - 1) & 1u, s_abort, err))) return false;
     const uint32_t abuf = a_base + b * a_stage_bytes(NMAT);
     const uint32_t off = abuf + (uint32_t)(((row >> 3) * 4 + quarter) * 128 + (row & 7) * 16);
-    // the chunk's 8 texels go out as two 8-byte halves (four texels each), so only two texel pairs'
-    // BF16 parts are held in registers at a time
+    // the chunk's 8 texels go out as two 8-byte halves of four texels each: one horizon vote per
+    // half (four texels below every lane's horizon get zero weights), then the four texels' weights
+    // side by side -- four independent chains, the builders being latency-bound
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
       uint32_t hi[NMAT][2], lo[NMAT][2];
+      const int tq = st * kStageT + quarter * 8 + half * 4;
+      float4 Aq[4];
+      float nlq[4];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int jj = half * 4 + h * 2;
-        const int t = st * kStageT + quarter * 8 + jj;
-        const float4 A0 = s_tab[2 * t];
-        const float4 A1 = s_tab[2 * t + 2];
-        const float nl0 = dot3(g.nx, g.ny, g.nz, A0.x, A0.y, A0.z);
-        const float nl1 = dot3(g.nx, g.ny, g.nz, A1.x, A1.y, A1.z);
-        if (!__any_sync(0xffffffffu, nl0 > 0.f || nl1 > 0.f)) {
+      for (int i = 0; i < 4; ++i) {
+        Aq[i] = s_tab[2 * (tq + i)];
+        nlq[i] = dot3(g.nx, g.ny, g.nz, Aq[i].x, Aq[i].y, Aq[i].z);
+      }
+      if (!__any_sync(0xffffffffu, nlq[0] > 0.f || nlq[1] > 0.f || nlq[2] > 0.f || nlq[3] > 0.f)) {
 #pragma unroll
-          for (int m = 0; m < NMAT; ++m) hi[m][h] = lo[m][h] = 0u;
-          continue;
+        for (int m = 0; m < NMAT; ++m) hi[m][0] = lo[m][0] = hi[m][1] = lo[m][1] = 0u;
+      } else {
+        float wdq[4], wsq[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float dwpi = s_tab[2 * (tq + i) + 1].w;
+          const float vq = pair_vis<VIS, ONEV>(w0, w1, w2, 1u << (half * 4 + i), g, cs);
+          pair_fwd_weights<DIFF, SPEC>(g, sc, Aq[i], dwpi, nlq[i], vq, wdq[i], wsq[i]);
         }
-        const float4 B0 = s_tab[2 * t + 1];
-        const float4 B1 = s_tab[2 * t + 3];
-        const float vis0 = pair_vis<VIS, ONEV>(w0, w1, w2, 1u << jj, g, cs);
-        const float vis1 = pair_vis<VIS, ONEV>(w0, w1, w2, 2u << jj, g, cs);
-        float wd0, ws0, wd1, ws1;
-        pair_fwd_weights<DIFF, SPEC>(g, sc, A0, B0.w, nl0, vis0, wd0, ws0);
-        pair_fwd_weights<DIFF, SPEC>(g, sc, A1, B1.w, nl1, vis1, wd1, ws1);
-        if (DIFF) split2(wd0, wd1, hi[0][h], lo[0][h]);
-        if (SPEC) split2(ws0, ws1, hi[NMAT - 1][h], lo[NMAT - 1][h]);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (DIFF) split2(wdq[2 * h], wdq[2 * h + 1], hi[0][h], lo[0][h]);
+          if (SPEC) split2(wsq[2 * h], wsq[2 * h + 1], hi[NMAT - 1][h], lo[NMAT - 1][h]);
+        }
       }
 #pragma unroll
       for (int m = 0; m < NMAT; ++m) {

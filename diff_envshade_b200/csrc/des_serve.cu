@@ -674,9 +674,10 @@ struct Req {
   double remaining() const {
     return (n_tiles - fwd_issued) * cost_fwd_tile + (in.backward ? (n_tiles - bwd_issued) * cost_bwd_tile : 0.0);
   }
-  // Scheduling key (lower goes first): the remaining work, or with rank_by_size the remaining
-  // points x texels, which ranks a request asking for gradients like the same request without.
-  bool rank_by_size = false;
+  // Scheduling key (lower goes first): with rank_by_size (the server's default) the remaining
+  // points x texels, which ranks a request asking for gradients like the same request without;
+  // otherwise the remaining work (an adjoint pair counts twice).
+  bool rank_by_size = true;
   double rank() const {
     if (!rank_by_size) return remaining();
     const int left = in.backward ? n_tiles - std::min(fwd_issued, bwd_issued) : n_tiles - fwd_issued;
@@ -841,7 +842,11 @@ struct des_server {
   std::vector<des::serve::Env> envs;
   std::vector<des::serve::Mesh> meshes;
   des::serve::Tick ticks[des::serve::kNTicks];
-  std::atomic<bool> rank_by_size{false};
+  // Ranking by size rather than by work: on the mixed serving workload (Poisson 5k/s, ten runs over
+  // five arrival seeds) it gave the 50k-100k-point class a p99 of 0.97 ms on average instead of
+  // 1.07 ms at the same throughput -- that class's slowest requests are the ones with gradients,
+  // which ranking by work puts behind forward requests of up to twice their size.
+  std::atomic<bool> rank_by_size{true};
   int sms = 0, grid = 0;
   size_t smem = 0;
 

@@ -240,10 +240,10 @@ int des_server_set_ticks_in_flight(des_server* s, int n);
  * are shaded; smaller ones are shaded in input order (by default no request is ordered).  Applies
  * to requests admitted after the call. */
 int des_server_set_order_min_points(des_server* s, int64_t n);
-/* Scheduling order of the ready requests (and of their uploads): least remaining work first
- * (enable = 0, the default), or least remaining points x texels first (enable = 1), which ranks a
- * request that asks for gradients like the same request without them.  Applies to requests
- * admitted after the call. */
+/* Scheduling order of the ready requests (and of their uploads): least remaining points x texels
+ * first (enable = 1, the default), which ranks a request that asks for gradients like the same
+ * request without them, or least remaining work first (enable = 0; an adjoint pair counts twice).
+ * Applies to requests admitted after the call. */
 int des_server_set_rank_by_size(des_server* s, int enable);
 int des_server_stats(des_server* s, des_serve_stats* out);
 /* Finishes queued work and frees the server. */
