@@ -679,7 +679,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_serve:
         # served p50/p99 against serial plain launches on one arrival schedule (2000 requests, Poisson 5k/s)
         from diff_envshade_b200 import serve_workload
-        serving = serve_workload.run(n=2000, rate=5000.0, tick_us=75)
+        serving = serve_workload.run(n=2000, rate=5000.0, tick_us=50)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -11,9 +11,10 @@
 //   * keeps env maps (their texel tables) and meshes (faces + visibility words) resident, shared by
 //     reference between requests;
 //   * every tick packs 32-point tiles of the ready requests, lowest rank first (remaining points x
-//     texels, or remaining work), up to a time budget, into a work list in mapped pinned memory and
-//     launches it as a CUDA graph (one persistent batch kernel) on its own stream, with up to
-//     ticks_in_flight ticks queued so that consecutive ticks overlap;
+//     texels, or remaining work), up to a time budget, into a work list, copies the list (and the
+//     descriptors of requests it names for the first time) to the device and launches it as a CUDA
+//     graph (one persistent batch kernel) on its own stream, with up to ticks_in_flight ticks
+//     queued so that consecutive ticks overlap;
 //   * when every tile of a request has finished, copies its outputs back (unless they were stored
 //     in place) and frees its memory.
 // Work of different requests therefore shares each launch and each SM; a request that arrives
@@ -35,6 +36,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstddef>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -118,9 +120,10 @@ struct WorkItem {
   int32_t req, tile, kind, pad;  // kind 0 = forward tile, 1 = adjoint tile
 };
 
-// One tick's work, written by the scheduler into pinned host memory that the GPU reads directly
-// (mapped), so a tick needs no host-to-device copy: the batch kernel fetches each item over the
-// host link while it computes the previous one.
+// One tick's work, written by the scheduler into pinned host memory and copied to the device ahead of
+// the tick's launch, on the tick's stream (n and the first n items), so that the batch kernel reads
+// its work items, the first ones included, from device memory.  `started` is the exception: the CTA
+// that claims item 0 sets it in the host copy (mapped), where the scheduler reads it.
 struct WorkList {
   unsigned n;        // items in the list (written by the scheduler)
   unsigned started;  // set to 1 by the CTA that claims item 0 (the tick is running)
@@ -457,11 +460,12 @@ __device__ __forceinline__ void dispatch_tile(const ReqDesc& r, int tile, const 
   }
 }
 
-// reqs: the slots' descriptors in mapped pinned host memory, written by the scheduler before the
-// first tick that names the slot; a CTA copies the descriptor of the request it works on into
-// shared memory (one read over the host link per change of request).  started: the work list's
-// flag that the CTA claiming item 0 sets (mapped; the scheduler reads it).  slot_tiles: per slot,
-// the adjoint tiles finished so far over all of the slot's requests (never reset).
+// reqs: the slots' descriptors in device memory, copied there by the scheduler on the stream of the
+// first tick that names the slot, before its launch; a CTA copies the descriptor of the request it
+// works on into shared memory (once per change of request).  wl: the tick's work list (device copy).
+// started: the work list's flag that the CTA claiming item 0 sets (mapped host memory; the
+// scheduler reads it).  slot_tiles: per slot, the adjoint tiles finished so far over all of the
+// slot's requests (never reset).
 __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __restrict__ reqs,
                                                             const WorkList* __restrict__ wl,
                                                             unsigned* started, TickCtl* ctl,
@@ -518,9 +522,8 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
       continue;
     }
     if (item.req != staged_req) {
-      // plain loads, as for the work list: the host writes a slot's descriptor before it launches
-      // the first tick that names the slot.  (Loads with the .cv qualifier, which refetch system
-      // memory lines, slowed the whole kernel down several times.)
+      // plain loads: the descriptor reached device memory before the launch of the first tick that
+      // names the slot (stream order), and stays unchanged while any tick names the slot
       constexpr int kWords = (int)(sizeof(ReqDesc) / 16);
       const uint4* src = reinterpret_cast<const uint4*>(reqs + item.req);
       uint4* dst = reinterpret_cast<uint4*>(&s_desc);
@@ -550,7 +553,18 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
         s_pf_kind[pb ^ 1] = next.kind;
       }
     }
-    const TilePoints* pts = pre ? &s_pts[pb] : nullptr;
+    // a tile in input order whose points were not prefetched (the CTA's first item of the tick, or
+    // the first after a change of request): the same copies into this item's buffer, completed
+    // before the tile starts, so that the warps read the 32 points from shared memory instead of
+    // each warp fetching all of them itself (over the host link for inputs read in place)
+    bool staged = pre;
+    if (!pre && r.perm == nullptr) {
+      prefetch_points(r, item.tile, item.kind == 1, &s_pts[pb]);
+      cp_async_wait_all();
+      __syncthreads();
+      staged = true;
+    }
+    const TilePoints* pts = staged ? &s_pts[pb] : nullptr;
     if (item.kind == 0) {
       dispatch_tile<true>(r, item.tile, s_tab, s_red, pts);
     } else {
@@ -671,6 +685,7 @@ struct Req {
   // ids, barycentrics, shading gradient, diffuse gradient), when inplace_in.
   bool inplace_in = false;
   const void* i[9] = {};
+  bool desc_sent = false;  // the descriptor has been queued for the device (with the first tick naming it)
   double remaining() const {
     return (n_tiles - fwd_issued) * cost_fwd_tile + (in.backward ? (n_tiles - bwd_issued) * cost_bwd_tile : 0.0);
   }
@@ -808,8 +823,9 @@ struct Mesh {
 };
 
 struct Tick {
-  WorkList* h = nullptr;  // pinned, mapped
-  WorkList* d = nullptr;  // the device's address of h
+  WorkList* h = nullptr;    // pinned, mapped: the scheduler writes the list here
+  WorkList* d = nullptr;    // the device's address of h (the kernel sets d->started)
+  WorkList* dev = nullptr;  // device copy of the list, which the kernel reads
   TickCtl* ctl = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t stream = nullptr;
@@ -823,7 +839,7 @@ struct Tick {
 
 struct des_server {
   int device = 0;
-  int tick_us = 75;
+  int tick_us = 50;
   std::atomic<int> ticks_in_flight{4};  // tick buffers in use at once (<= kNTicks)
   double pairs_per_us = 0;              // the batch kernel's throughput, which sizes the ticks
   std::atomic<int64_t> order_min_p{des::serve::kServeOrderMinP};  // requests with fewer points are shaded in input order
@@ -832,8 +848,8 @@ struct des_server {
   unsigned char* arena_base = nullptr;
   des::serve::Arena arena;
   unsigned* d_ctrl = nullptr;
-  des::serve::ReqDesc* h_desc = nullptr;  // per slot, mapped pinned host memory
-  des::serve::ReqDesc* d_desc = nullptr;  // the device's address of h_desc
+  des::serve::ReqDesc* h_desc = nullptr;  // per slot, pinned host memory (written at admission)
+  des::serve::ReqDesc* d_desc = nullptr;  // per slot, device copy (sent with the slot's first tick)
   unsigned* d_slot_tiles = nullptr;       // per slot, adjoint tiles finished (device, never reset)
   std::vector<unsigned> slot_tiles_base;  // per slot, the counter's value once its requests are done
   std::vector<double*> acc_pool;          // zeroed FP64 env-gradient accumulators, 3 x kMaxHWpad each
@@ -1121,7 +1137,7 @@ bool upload(des_server* s, Req* r) {
     s->slot_tiles_base[r->slot] += (unsigned)r->n_tiles;  // wraps like the device counter
     d.bwd_target = s->slot_tiles_base[r->slot];
   }
-  // the descriptor goes to mapped host memory; the batch kernel reads it from there
+  // the descriptor goes to the device with the first tick that names the slot (launch_tick)
   s->h_desc[r->slot] = d;
   if (job->segs.empty()) {  // inputs read in place: nothing to copy
     delete job;
@@ -1263,11 +1279,28 @@ bool launch_tick(des_server* s) {
   }
   t->h->n = n;
   t->h->started = 0u;
-  std::atomic_thread_fence(std::memory_order_seq_cst);  // items are in host memory before the launch
+  std::atomic_thread_fence(std::memory_order_seq_cst);  // items are in host memory before the copies
+  // ahead of the kernel on the tick's stream: the descriptors of the slots this tick names for the
+  // first time, then the list.  A later tick is launched only once this one has started, i.e. after
+  // these copies completed, so every tick finds the descriptors of all the slots it names.
+  bool copied = true;
+  for (auto& c : t->counts) {
+    Req* r = c.first;
+    if (r->desc_sent) continue;
+    copied = copied && cudaMemcpyAsync(s->d_desc + r->slot, s->h_desc + r->slot, sizeof(ReqDesc),
+                                       cudaMemcpyHostToDevice, t->stream) == cudaSuccess;
+    r->desc_sent = true;
+  }
+  copied = copied && cudaMemcpyAsync(t->dev, t->h, offsetof(WorkList, items) + (size_t)n * sizeof(WorkItem),
+                                     cudaMemcpyHostToDevice, t->stream) == cudaSuccess;
+  if (!copied) {  // nothing launched; the worker fails the outstanding requests
+    s->failed = true;
+    return false;
+  }
   if (cudaGraphLaunch(t->exec, t->stream) != cudaSuccess) {
     // launch the same work without the graph
     cudaGetLastError();
-    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_desc, t->d, &t->d->started, t->ctl,
+    batch_kernel<<<s->grid, kNW * 32, s->smem, t->stream>>>(s->d_desc, t->dev, &t->d->started, t->ctl,
                                                             s->d_slot_tiles, s->d_ctrl);
     s->stats.device_error |= 16;
   }
@@ -1485,9 +1518,9 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
             s->down.init(cudaMemcpyDeviceToHost, size_t(1) << 20, size_t(4) << 20) && s->order.init() &&
             cudaMalloc(&s->arena_base, hbm_budget_bytes) == cudaSuccess &&
             cudaMalloc(&s->d_ctrl, 256) == cudaSuccess &&
-            cudaHostAlloc(&s->h_desc, sizeof(des::serve::ReqDesc) * des::serve::kMaxSlots, cudaHostAllocMapped) ==
+            cudaHostAlloc(&s->h_desc, sizeof(des::serve::ReqDesc) * des::serve::kMaxSlots, cudaHostAllocDefault) ==
                 cudaSuccess &&
-            cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_desc), s->h_desc, 0) == cudaSuccess &&
+            cudaMalloc(&s->d_desc, sizeof(des::serve::ReqDesc) * des::serve::kMaxSlots) == cudaSuccess &&
             cudaMalloc(&s->d_slot_tiles, sizeof(unsigned) * des::serve::kMaxSlots) == cudaSuccess &&
             cudaMemset(s->d_slot_tiles, 0, sizeof(unsigned) * des::serve::kMaxSlots) == cudaSuccess &&
             cudaMemset(s->d_ctrl, 0, 256) == cudaSuccess;
@@ -1515,6 +1548,7 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
   for (auto& t : s->ticks) {
     ok = cudaHostAlloc(&t.h, sizeof(des::serve::WorkList), cudaHostAllocMapped) == cudaSuccess &&
          cudaHostGetDevicePointer(reinterpret_cast<void**>(&t.d), t.h, 0) == cudaSuccess &&
+         cudaMalloc(&t.dev, sizeof(des::serve::WorkList)) == cudaSuccess &&
          cudaMalloc(&t.ctl, sizeof(des::serve::TickCtl)) == cudaSuccess &&
          cudaMemset(t.ctl, 0, sizeof(des::serve::TickCtl)) == cudaSuccess &&
          cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking) == cudaSuccess &&
@@ -1528,7 +1562,7 @@ int des_server_create(int device, size_t hbm_budget_bytes, int tick_us, des_serv
     cudaGraph_t g = nullptr;
     ok = cudaStreamBeginCapture(t.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     des::serve::batch_kernel<<<s->grid, des::serve::kNW * 32, s->smem, t.stream>>>(
-        s->d_desc, t.d, &t.d->started, t.ctl, s->d_slot_tiles, s->d_ctrl);
+        s->d_desc, t.dev, &t.d->started, t.ctl, s->d_slot_tiles, s->d_ctrl);
     ok = ok && cudaStreamEndCapture(t.stream, &g) == cudaSuccess;
     ok = ok && cudaGraphInstantiate(&t.exec, g, 0) == cudaSuccess;
     if (g) cudaGraphDestroy(g);
@@ -1678,6 +1712,7 @@ int des_server_destroy(des_server* s) {
   for (auto& t : s->ticks) {
     if (t.exec) cudaGraphExecDestroy(t.exec);
     if (t.h) cudaFreeHost(t.h);
+    if (t.dev) cudaFree(t.dev);
     if (t.ctl) cudaFree(t.ctl);
     if (t.done) cudaEventDestroy(t.done);
     if (t.stream) cudaStreamDestroy(t.stream);
@@ -1690,6 +1725,7 @@ int des_server_destroy(des_server* s) {
   for (Req* r : s->pending) delete r;
   for (Req* r : s->incoming) delete r;
   if (s->h_desc) cudaFreeHost(s->h_desc);
+  if (s->d_desc) cudaFree(s->d_desc);
   if (s->d_slot_tiles) cudaFree(s->d_slot_tiles);
   for (void* c : s->acc_chunks) cudaFree(c);
   if (s->d_ctrl) cudaFree(s->d_ctrl);

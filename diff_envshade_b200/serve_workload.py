@@ -101,7 +101,7 @@ def _summarize(lat_s, sched, makespan_s):
     return out
 
 
-def run_served(pools, sched, bary, device=0, hbm_budget_bytes=40 << 30, tick_us=75, ticks_in_flight=None,
+def run_served(pools, sched, bary, device=0, hbm_budget_bytes=40 << 30, tick_us=50, ticks_in_flight=None,
                trace=False, order_min_points=None, rank_by_size=None):
     from .serving import Server
     srv = Server(device=device, hbm_budget_bytes=hbm_budget_bytes, tick_us=tick_us, ticks_in_flight=ticks_in_flight,
@@ -218,7 +218,7 @@ def run_serial_plain(pools, sched, bary, device=0):
     return _summarize(lat, sched, makespan)
 
 
-def run(n=2000, rate=5000.0, tick_us=75, serial=True, hbm_budget_bytes=40 << 30, seed=7, ticks_in_flight=None):
+def run(n=2000, rate=5000.0, tick_us=50, serial=True, hbm_budget_bytes=40 << 30, seed=7, ticks_in_flight=None):
     """Both arms on one arrival schedule; returns {"served": ..., "serial_plain": ...}."""
     pools = Pools()
     sched = make_schedule(n=n, rate=rate, seed=seed)
@@ -232,7 +232,7 @@ def run(n=2000, rate=5000.0, tick_us=75, serial=True, hbm_budget_bytes=40 << 30,
     return res
 
 
-def run_single(P, vis=False, backward=False, reps=2, H=16, W=32, tick_us=75, seed=4242, where="host",
+def run_single(P, vis=False, backward=False, reps=2, H=16, W=32, tick_us=50, seed=4242, where="host",
                order_min_points=None):
     """One request shape submitted `reps` times, one after the other, to an otherwise idle server:
     each one's compute time (ready -> last tile done, ms) and the ticks it took.  For timing and
@@ -282,7 +282,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=2000)
     ap.add_argument("--rate", type=float, default=5000.0)
-    ap.add_argument("--tick-us", type=int, default=75)
+    ap.add_argument("--tick-us", type=int, default=50)
     ap.add_argument("--seed", type=int, default=7, help="seed of the arrival schedule")
     ap.add_argument("--ticks-in-flight", type=int, default=None)
     ap.add_argument("--no-serial", action="store_true")

@@ -3,7 +3,7 @@
 The scheduler itself is native (a C++ thread inside libdes_b200.so): this module only binds the C
 ABI with ctypes (calls release the GIL) and manages the host tensors a request points at.
 
-    srv = Server(device=0, hbm_budget_bytes=40 << 30, tick_us=75)
+    srv = Server(device=0, hbm_budget_bytes=40 << 30, tick_us=50)
     env = srv.add_envmap(envmap_3xHxW, rotation_3x3)
     mesh = srv.add_mesh(face_vertex_list_3xF_int32, visibility_SxV_int32)
     req = srv.submit(normal, view_dir, albedo, specular_albedo, roughness, env_id=env, mesh_id=mesh,
@@ -108,7 +108,7 @@ class Request:
 
 
 class Server:
-    def __init__(self, device=0, hbm_budget_bytes=40 << 30, tick_us=75, ticks_in_flight=None,
+    def __init__(self, device=0, hbm_budget_bytes=40 << 30, tick_us=50, ticks_in_flight=None,
                  order_min_points=None, rank_by_size=None):
         self._L = _load()
         h = _vp()
