@@ -484,8 +484,8 @@ __global__ void __launch_bounds__(kNW * 32, 2) batch_kernel(const ReqDesc* __res
   int staged_req = -1;
   const float4* staged_table = nullptr;
   // Work items go through a ring of three: while the CTA computes item `it`, item it+1 is already
-  // in shared memory (its points are being prefetched), and thread 0 copies item it+2 in with
-  // cp.async (the work list is mapped host memory) and claims the index after it.  Every thread
+  // in shared memory (its points are being prefetched), and thread 0 copies item it+2 in from the
+  // device copy of the work list with cp.async and claims the index after it.  Every thread
   // waits for its own copies just before the barrier that ends the iteration.
   int claimed = 0;
   if (threadIdx.x == 0) {
@@ -1034,8 +1034,9 @@ void resolve_request(des_server* s, Req* r) {
   r->inplace_in = in_ok;
 }
 
-// Lays out the request's buffers in its arena range, writes its descriptor (mapped host memory)
-// and queues its point data on the upload lane in prioritised slices.
+// Lays out the request's buffers in its arena range, writes its descriptor (pinned host memory; it
+// reaches the device with the first tick that names the slot) and queues its point data on the
+// upload lane in prioritised slices.
 // Returns false when the request has nothing to upload (it is ready right away).
 bool upload(des_server* s, Req* r) {
   const des_serve_request& q = r->in;
