@@ -40,6 +40,19 @@
 
 namespace des {
 
+// Programmatic dependent launch (sm_90+): every kernel of the path lets the next kernel in its stream
+// be scheduled as soon as all of its own CTAs are running (launch_dependents; the next kernel can
+// only be launched once every CTA of this one has started, so a waiting kernel never holds the
+// resources a running one still needs), then waits until its predecessor has completed and its
+// writes are visible (wait) before it touches global memory.  The next kernel's launch and CTA
+// start-up overlap this kernel's tail; a predecessor that does not take part (any other kernel in
+// the stream) simply completes first, as without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+
 // ------------------------------------------------------------------------------------------
 // Texel table
 // ------------------------------------------------------------------------------------------
@@ -82,6 +95,7 @@ __device__ __forceinline__ void table_entry(int t, int H, int W, const float* __
 __global__ void des_table_kernel(int H, int W, int HWpad, const float* __restrict__ R,
                                  const float* __restrict__ env, float4* __restrict__ rec,
                                  float* __restrict__ export4, unsigned* __restrict__ ctrl) {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0 && ctrl != nullptr) {
     ctrl[kCtrlTileCounter] = 0u;
@@ -146,6 +160,7 @@ __global__ void __launch_bounds__(kSortThreads, 1) des_prep_kernel(int H, int W,
                                                                 int chunk, int ncp, unsigned* __restrict__ counts,
                                                                 uint16_t* __restrict__ keys,
                                                                 uint32_t* __restrict__ rank) {
+  pdl_enter();
   constexpr int NW = kSortThreads / 32;
   constexpr int SUB = 2 * kSortThreads;  // points per pass: 2 rounds per warp
   __shared__ uint16_t cnt[NW][kSortBins];
@@ -231,6 +246,7 @@ __global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chu
                                                               const uint16_t* __restrict__ keys,
                                                               const uint32_t* __restrict__ rank,
                                                               int32_t* __restrict__ perm) {
+  pdl_enter();
   __shared__ unsigned off[kSortBins];
   __shared__ unsigned warp_tot[kSortBins / 32];
   const int k = threadIdx.x, lane = k & 31, w = k >> 5;
@@ -330,6 +346,7 @@ __device__ __forceinline__ void fwd_tile_sums(const ShadeParams& p, const PointG
 
 template <bool DIFF, bool SPEC, bool VIS>
 __global__ void __maxnreg__(64) des_fwd_kernel(const ShadeParams p) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* s_tab = reinterpret_cast<float4*>(smem_raw);
   float* s_red = reinterpret_cast<float*>(smem_raw + (size_t)p.chunk * 32);
@@ -444,6 +461,7 @@ __device__ __forceinline__ void bwd_tile_sums(const ShadeParams& p, const PointG
 
 template <bool DIFF, bool SPEC, bool VIS>
 __global__ void __launch_bounds__(kMaxThreads, 1) des_bwd_kernel(const ShadeParams p) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* s_tab = reinterpret_cast<float4*>(smem_raw);
   double* s_env = reinterpret_cast<double*>(smem_raw + (size_t)p.chunk * 32);  // [3][chunk], single chunk
@@ -541,6 +559,7 @@ constexpr int kReduceCols = 8, kReduceRows = 128;
 __global__ void __launch_bounds__(kReduceCols* kReduceRows) des_env_reduce_kernel(const double* __restrict__ partial,
                                                                                   int nparts, int HW, int HWpad,
                                                                                   float* __restrict__ g_env) {
+  pdl_enter();
   __shared__ double s[kReduceRows][kReduceCols + 1];
   const int x = threadIdx.x, y = threadIdx.y;
   const int k = blockIdx.x * kReduceCols + x;  // index into [3][HWpad]
@@ -619,6 +638,24 @@ int occupancy(K kernel, int threads, size_t smem) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess) return 0;
   occ_cache[key] = nb;
   return nb;
+}
+
+// Launches `kernel` on (grid, block, smem, stream) with programmatic stream serialization (the
+// kernels of this file call pdl_enter() first).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 using KernelFn = void (*)(const ShadeParams);
@@ -801,14 +838,14 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   if (reuse_table) {
     // nothing to launch before the adjoint
   } else if (sort && !reuse) {
-    des_prep_kernel<<<lp.sort_chunks, kSortThreads, 0, stream>>>(a.H, a.W, lp.HWpad, a.light2obj_rotmat, a.envmap,
-                                                                 table, ctrl, a.normal, a.P, lp.sort_chunk,
-                                                                 sort_row(lp), sort_counts, sort_keys, sort_rank);
+    launch_pdl(des_prep_kernel, dim3(lp.sort_chunks), dim3(kSortThreads), 0, stream, a.H, a.W, lp.HWpad,
+               a.light2obj_rotmat, a.envmap, table, ctrl, a.normal, a.P, lp.sort_chunk, sort_row(lp), sort_counts,
+               sort_keys, sort_rank);
   } else {
     const int threads = 256;
     const int blocks = (lp.HWpad + threads - 1) / threads;
-    des_table_kernel<<<blocks, threads, 0, stream>>>(a.H, a.W, lp.HWpad, a.light2obj_rotmat, a.envmap, table,
-                                                     nullptr, ctrl);
+    launch_pdl(des_table_kernel, dim3(blocks), dim3(threads), 0, stream, a.H, a.W, lp.HWpad, a.light2obj_rotmat,
+               a.envmap, table, nullptr, ctrl);
   }
   if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
   if (!reuse_table) count_launches(1);
@@ -868,8 +905,8 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   prm.env_in_smem = lp.env_in_smem;
   prm.perm = nullptr;
   if (sort && !reuse) {
-    des_place_kernel<<<lp.sort_chunks, kSortBins, 0, stream>>>(a.P, lp.sort_chunk, lp.sort_chunks, sort_row(lp),
-                                                               sort_counts, sort_keys, sort_rank, perm);
+    launch_pdl(des_place_kernel, dim3(lp.sort_chunks), dim3(kSortBins), 0, stream, a.P, lp.sort_chunk,
+               lp.sort_chunks, sort_row(lp), sort_counts, sort_keys, sort_rank, perm);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
     count_launches(1);
   }
@@ -878,7 +915,7 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   KernelFn k = call.backward ? pick<BwdSel>(diff, spec, vis) : pick<FwdSel>(diff, spec, vis);
   cudaEvent_t ev0 = g_timing_start.load(), ev1 = g_timing_stop.load();
   if (ev0 != nullptr && ev1 != nullptr) cudaEventRecord(ev0, stream);
-  k<<<grid, lp.nw * 32, lp.smem, stream>>>(prm);
+  launch_pdl(k, dim3(grid), dim3(lp.nw * 32), lp.smem, stream, prm);
   if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
   count_launches(1);
   if (ev0 != nullptr && ev1 != nullptr) cudaEventRecord(ev1, stream);
@@ -886,7 +923,8 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   if (call.backward && call.g_envmap != nullptr) {
     const dim3 rb(kReduceCols, kReduceRows);
     const int rg = (3 * lp.HWpad + kReduceCols - 1) / kReduceCols;
-    des_env_reduce_kernel<<<rg, rb, 0, stream>>>(env_partial, grid, a.H * a.W, lp.HWpad, call.g_envmap);
+    launch_pdl(des_env_reduce_kernel, dim3(rg), dim3(rb), 0, stream, env_partial, grid, a.H * a.W, lp.HWpad,
+               call.g_envmap);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
     count_launches(1);
   }
@@ -908,9 +946,10 @@ int launch_point_order(const float* normal, int64_t P, void* scratch, int32_t* p
                                                align_up((size_t)kSortBins * ncp * sizeof(unsigned), 256));
   uint32_t* rank = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(keys) +
                                                align_up((size_t)P * sizeof(uint16_t), 256));
-  des_prep_kernel<<<nchunks, kSortThreads, 0, stream>>>(0, 0, 0, nullptr, nullptr, nullptr, nullptr, normal, P, chunk,
-                                                        ncp, counts, keys, rank);
-  des_place_kernel<<<nchunks, kSortBins, 0, stream>>>(P, chunk, nchunks, ncp, counts, keys, rank, perm);
+  launch_pdl(des_prep_kernel, dim3(nchunks), dim3(kSortThreads), 0, stream, 0, 0, 0, nullptr, nullptr, nullptr, nullptr,
+             normal, P, chunk, ncp, counts, keys, rank);
+  launch_pdl(des_place_kernel, dim3(nchunks), dim3(kSortBins), 0, stream, P, chunk, nchunks, ncp, counts, keys, rank,
+             perm);
   count_launches(2);
   return cudaGetLastError() == cudaSuccess ? DES_OK : DES_ERR_CUDA;
 }
@@ -918,7 +957,8 @@ int launch_point_order(const float* normal, int64_t P, void* scratch, int32_t* p
 int launch_table(int H, int W, int HWpad, const float* R, const float* env, float4* rec, unsigned* ctrl,
                  cudaStream_t stream) {
   const int threads = 256;
-  des_table_kernel<<<(HWpad + threads - 1) / threads, threads, 0, stream>>>(H, W, HWpad, R, env, rec, nullptr, ctrl);
+  launch_pdl(des_table_kernel, dim3((HWpad + threads - 1) / threads), dim3(threads), 0, stream, H, W, HWpad, R, env,
+             rec, nullptr, ctrl);
   count_launches(1);
   return cudaGetLastError() == cudaSuccess ? DES_OK : DES_ERR_CUDA;
 }
@@ -927,8 +967,8 @@ int launch_texel_table(int H, int W, const float* R, float* out, des_stream_t st
   cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   const int HWpad = (H * W + 31) / 32 * 32;
   const int threads = 256;
-  des_table_kernel<<<(HWpad + threads - 1) / threads, threads, 0, stream>>>(H, W, HWpad, R, nullptr, nullptr, out,
-                                                                            nullptr);
+  launch_pdl(des_table_kernel, dim3((HWpad + threads - 1) / threads), dim3(threads), 0, stream, H, W, HWpad, R,
+             nullptr, nullptr, out, nullptr);
   count_launches(1);
   return cudaGetLastError() == cudaSuccess ? DES_OK : DES_ERR_CUDA;
 }
