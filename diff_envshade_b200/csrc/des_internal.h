@@ -4,6 +4,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "diff_envshade_b200.h"
 
 namespace des {
@@ -23,6 +25,38 @@ inline int sort_chunk_for(int64_t P) {
   int chunk = kSortMinChunk;
   while ((int64_t)chunk * kSortMaxChunks < P) chunk *= 2;
   return chunk;
+}
+
+// Programmatic dependent launch (sm_90+): every kernel launched with launch_pdl() starts with
+// pdl_enter(), which lets the next kernel in its stream be scheduled as soon as all of its own CTAs
+// are running (launch_dependents; the next kernel can only be launched once every CTA of this one
+// has started, so a waiting kernel never holds the resources a running one still needs), then
+// waits until its predecessor has completed and its writes are visible (wait) before it touches
+// global memory.  The next kernel's launch and CTA start-up overlap this kernel's tail; a
+// predecessor that does not take part (any other kernel in the stream) simply completes first, as
+// without the attribute.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+#endif
+
+// Launches `kernel` on (grid, block, smem, stream) with programmatic stream serialization.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // control words at the start of every workspace

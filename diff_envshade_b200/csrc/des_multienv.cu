@@ -227,6 +227,7 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_
 // and the block): per stage one [3 kpad x 32] B operand, rows ordered by colour channel, then env map.
 __global__ void prep_kernel(const float* __restrict__ env, int HW, int nst, int kbase, int kblock, int kpad,
                             uint8_t* __restrict__ bprep) {
+  pdl_enter();
   const int ncols = 3 * kpad;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // over nst * ncols * 32
   const int total = nst * ncols * kStageT;
@@ -328,6 +329,7 @@ __device__ __forceinline__ bool build_tile(const Params& p, const float4* s_tab,
 
 template <bool DIFF, bool SPEC, bool VIS>
 __global__ void __launch_bounds__(kThreads, 1) relight_kernel(const Params p) {
+  pdl_enter();
   constexpr int NMAT = (DIFF ? 1 : 0) + (SPEC ? 1 : 0);
   extern __shared__ __align__(1024) uint8_t smem[];
   const int HWpad = p.pt.HWpad;
@@ -691,8 +693,8 @@ int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigne
     const relight::Smem L = relight::smem_layout(HWpad, prm.kpad, prm.nmat, prm.nstage);
     if ((int)L.total > max_smem) return DES_ERR_UNSUPPORTED;
     const int total = prm.nst * prm.ncols * relight::kStageT;
-    relight::prep_kernel<<<(total + 255) / 256, 256, 0, stream>>>(envmaps, HW, prm.nst, kbase, prm.kblock, prm.kpad,
-                                                                  bprep);
+    launch_pdl(relight::prep_kernel, dim3((total + 255) / 256), dim3(256), 0, stream, envmaps, HW, prm.nst, kbase,
+               prm.kblock, prm.kpad, bprep);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total) != cudaSuccess)
       return DES_ERR_CUDA;
@@ -700,7 +702,7 @@ int launch_relight(const des_shade_args& a, const float* envmaps, int K, unsigne
     timing_events(ev0, ev1);
     const bool timed = ev0 != nullptr && ev1 != nullptr && kbase == 0;  // the first pass of K
     if (timed) cudaEventRecord(ev0, stream);
-    k<<<grid, relight::kThreads, L.total, stream>>>(prm);
+    launch_pdl(k, dim3(grid), dim3(relight::kThreads), L.total, stream, prm);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
     if (timed) cudaEventRecord(ev1, stream);
     count_launches(2);

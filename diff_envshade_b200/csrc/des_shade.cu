@@ -40,17 +40,6 @@
 
 namespace des {
 
-// Programmatic dependent launch (sm_90+): every kernel of the path lets the next kernel in its stream
-// be scheduled as soon as all of its own CTAs are running (launch_dependents; the next kernel can
-// only be launched once every CTA of this one has started, so a waiting kernel never holds the
-// resources a running one still needs), then waits until its predecessor has completed and its
-// writes are visible (wait) before it touches global memory.  The next kernel's launch and CTA
-// start-up overlap this kernel's tail; a predecessor that does not take part (any other kernel in
-// the stream) simply completes first, as without the attribute.
-__device__ __forceinline__ void pdl_enter() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-}
 
 
 // ------------------------------------------------------------------------------------------
@@ -638,24 +627,6 @@ int occupancy(K kernel, int threads, size_t smem) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess) return 0;
   occ_cache[key] = nb;
   return nb;
-}
-
-// Launches `kernel` on (grid, block, smem, stream) with programmatic stream serialization (the
-// kernels of this file call pdl_enter() first).
-template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
-                       Args&&... args) {
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 using KernelFn = void (*)(const ShadeParams);
