@@ -90,3 +90,43 @@ def test_next_call_waits_for_the_adjoints_env_reduction(des, d):
         torch.cuda.synchronize()
         for a, b in zip(got, want):
             assert torch.equal(a, b)
+
+
+def test_graph_replay_matches_eager_calls(des, d):
+    # the operator pair captured in a CUDA graph (its kernels become programmatic dependencies of
+    # one another) and replayed on changed inputs gives what eager calls give on the same inputs
+    normal = d.normal.clone()
+    gsh = d.grad_shading.clone()
+
+    def step():
+        sh, wh = des.bruteforce_specularvisibility_shader_forward2(*_base(d, normal), *_vis(d), True)
+        g = des.bruteforce_specularvisibility_shader_backward2(gsh, d.grad_diffuse_shading, *_base(d, normal),
+                                                               *_vis(d), True)
+        return [sh, wh] + list(g)
+
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            step()
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        outs = step()
+    for k in range(3):
+        normal.copy_(torch.roll(d.normal, shifts=k + 1, dims=0))
+        gsh.copy_(torch.roll(d.grad_shading, shifts=2 * k + 1, dims=0))
+        torch.autograd.graph.increment_version(normal)
+        graph.replay()
+        torch.cuda.synchronize()
+        want = des.bruteforce_specularvisibility_shader_forward2(*_base(d, normal.clone()), *_vis(d), True)
+        wg = des.bruteforce_specularvisibility_shader_backward2(gsh.clone(), d.grad_diffuse_shading,
+                                                                *_base(d, normal.clone()), *_vis(d), True)
+        torch.cuda.synchronize()
+        want = list(want) + list(wg)
+        for got, w in zip(outs[:7], want[:7]):
+            assert torch.equal(got, w)
+        scale = float(want[7].abs().max())
+        assert float((outs[7] - want[7]).abs().max()) <= 1e-6 * scale
+    del graph
