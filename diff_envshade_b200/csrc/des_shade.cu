@@ -139,14 +139,15 @@ __device__ __forceinline__ int normal_key(const float* __restrict__ normal, int6
 // cells rank themselves with __match_any_sync against the warp's own per-cell counters.  An
 // exclusive prefix of those counters over the warps then gives every point its rank among the
 // chunk's points of its cell (input order when the chunk is one pass of 1024 points; otherwise
-// warp by warp -- a fixed order either way, so the permutation is deterministic).  Outputs: keys[p] = cell, rank[p] = rank, and the chunk's cell
-// counts in column c of counts[k][ncp] (row length ncp = nchunks rounded up to 4).
+// warp by warp -- a fixed order either way, so the permutation is deterministic).  Outputs:
+// keys[p] = cell, rank[p] = rank, and the chunk's cell counts in row c of counts[chunk][cell]
+// (one coalesced 4 KB row per CTA).
 // Threads of every CTA also build the texel records (grid-stride over the table).
 __global__ void __launch_bounds__(kSortThreads, 1) des_prep_kernel(int H, int W, int HWpad, const float* __restrict__ R,
                                                                 const float* __restrict__ env,
                                                                 float4* __restrict__ rec, unsigned* __restrict__ ctrl,
                                                                 const float* __restrict__ normal, int64_t P,
-                                                                int chunk, int ncp, unsigned* __restrict__ counts,
+                                                                int chunk, unsigned* __restrict__ counts,
                                                                 uint16_t* __restrict__ keys,
                                                                 uint32_t* __restrict__ rank) {
   pdl_enter();
@@ -201,9 +202,7 @@ __global__ void __launch_bounds__(kSortThreads, 1) des_prep_kernel(int H, int W,
       cnt[q][k] = (uint16_t)run;
       run += c;
     }
-    counts[(size_t)k * ncp + blockIdx.x] = run;
-    if ((int)blockIdx.x == gridDim.x - 1)  // the padding columns of the row are zero
-      for (int q = gridDim.x; q < ncp; ++q) counts[(size_t)k * ncp + q] = 0u;
+    counts[(size_t)blockIdx.x * kSortBins + k] = run;
   }
   __syncthreads();
   if (nsub == 1) {
@@ -226,11 +225,12 @@ __global__ void __launch_bounds__(kSortThreads, 1) des_prep_kernel(int H, int W,
   }
 }
 
-// Ordering, step 2.  CTA c: thread k reads row k of counts (cell k's count in every chunk) and
-// sums it over all chunks (total) and over the chunks before c (prefix); a block scan of the
-// totals gives the first position of cell k; then every point p of chunk c goes to
-// perm[first(k) + prefix_c(k) + rank[p]]: cells in order, chunks in order within a cell.
-__global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chunk, int nchunks, int ncp,
+// Ordering, step 2.  CTA c: thread k reads column k of counts (cell k's count in every chunk; the
+// warp's reads of one row are coalesced) and sums it over all chunks (total) and over the chunks
+// before c (prefix); a block scan of the totals gives the first position of cell k; then every
+// point p of chunk c goes to perm[first(k) + prefix_c(k) + rank[p]]: cells in order, chunks in
+// order within a cell.
+__global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chunk, int nchunks,
                                                               const unsigned* __restrict__ counts,
                                                               const uint16_t* __restrict__ keys,
                                                               const uint32_t* __restrict__ rank,
@@ -240,20 +240,15 @@ __global__ void __launch_bounds__(kSortBins) des_place_kernel(int64_t P, int chu
   __shared__ unsigned warp_tot[kSortBins / 32];
   const int k = threadIdx.x, lane = k & 31, w = k >> 5;
   const int c = blockIdx.x;
-  const uint4* row = reinterpret_cast<const uint4*>(counts + (size_t)k * ncp);
-  // the row's padding columns (from nchunks to ncp) hold zeros
-  const int nq = ncp / 4, cq = c >> 2, cr = c & 3;
   unsigned pre = 0, tot = 0;
-  for (int q0 = 0; q0 < nq; q0 += 8) {
-    uint4 v[8];
+  for (int c0 = 0; c0 < nchunks; c0 += 8) {
+    unsigned v[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = (q0 + j < nq) ? row[q0 + j] : make_uint4(0u, 0u, 0u, 0u);
+    for (int j = 0; j < 8; ++j) v[j] = (c0 + j < nchunks) ? counts[(size_t)(c0 + j) * kSortBins + k] : 0u;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const unsigned sq = (v[j].x + v[j].y) + (v[j].z + v[j].w);
-      tot += sq;
-      if (q0 + j < cq) pre += sq;
-      if (q0 + j == cq) pre += (cr > 0 ? v[j].x : 0u) + (cr > 1 ? v[j].y : 0u) + (cr > 2 ? v[j].z : 0u);
+      tot += v[j];
+      if (c0 + j < c) pre += v[j];
     }
   }
   unsigned incl = tot;
@@ -649,7 +644,7 @@ struct BwdSel {
 };
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-// Row length of the [cell][chunk] count table: chunks rounded up to a multiple of 4 (16-byte rows).
+// Rows allocated for the [chunk][cell] count table: the chunks, rounded up to a multiple of 4.
 inline int sort_row(const LaunchPlan& lp) { return (lp.sort_chunks + 3) / 4 * 4; }
 
 }  // namespace
@@ -706,7 +701,7 @@ LaunchPlan plan_launch(int64_t P, int H, int W, bool backward, int dev, bool com
 size_t sort_area_bytes(const LaunchPlan& lp) {
   if (!lp.sort) return 0;
   return align_up((size_t)lp.ntiles * 32 * sizeof(int32_t), 256) +             // permutation
-         align_up((size_t)kSortBins * sort_row(lp) * sizeof(unsigned), 256) +  // cell counts [cell][chunk]
+         align_up((size_t)kSortBins * sort_row(lp) * sizeof(unsigned), 256) +  // cell counts [chunk][cell]
          align_up((size_t)lp.ntiles * 32 * sizeof(uint16_t), 256) +            // cell of each point
          align_up((size_t)lp.ntiles * 32 * sizeof(uint32_t), 256);             // rank of each point
 }
@@ -810,8 +805,8 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
     // nothing to launch before the adjoint
   } else if (sort && !reuse) {
     launch_pdl(des_prep_kernel, dim3(lp.sort_chunks), dim3(kSortThreads), 0, stream, a.H, a.W, lp.HWpad,
-               a.light2obj_rotmat, a.envmap, table, ctrl, a.normal, a.P, lp.sort_chunk, sort_row(lp), sort_counts,
-               sort_keys, sort_rank);
+               a.light2obj_rotmat, a.envmap, table, ctrl, a.normal, a.P, lp.sort_chunk, sort_counts, sort_keys,
+               sort_rank);
   } else {
     const int threads = 256;
     const int blocks = (lp.HWpad + threads - 1) / threads;
@@ -877,7 +872,7 @@ int launch_shade(const ShadeCall& call, des_stream_t stream_) {
   prm.perm = nullptr;
   if (sort && !reuse) {
     launch_pdl(des_place_kernel, dim3(lp.sort_chunks), dim3(kSortBins), 0, stream, a.P, lp.sort_chunk,
-               lp.sort_chunks, sort_row(lp), sort_counts, sort_keys, sort_rank, perm);
+               lp.sort_chunks, sort_counts, sort_keys, sort_rank, perm);
     if (cudaGetLastError() != cudaSuccess) return DES_ERR_CUDA;
     count_launches(1);
   }
@@ -918,9 +913,8 @@ int launch_point_order(const float* normal, int64_t P, void* scratch, int32_t* p
   uint32_t* rank = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(keys) +
                                                align_up((size_t)P * sizeof(uint16_t), 256));
   launch_pdl(des_prep_kernel, dim3(nchunks), dim3(kSortThreads), 0, stream, 0, 0, 0, nullptr, nullptr, nullptr, nullptr,
-             normal, P, chunk, ncp, counts, keys, rank);
-  launch_pdl(des_place_kernel, dim3(nchunks), dim3(kSortBins), 0, stream, P, chunk, nchunks, ncp, counts, keys, rank,
-             perm);
+             normal, P, chunk, counts, keys, rank);
+  launch_pdl(des_place_kernel, dim3(nchunks), dim3(kSortBins), 0, stream, P, chunk, nchunks, counts, keys, rank, perm);
   count_launches(2);
   return cudaGetLastError() == cudaSuccess ? DES_OK : DES_ERR_CUDA;
 }
